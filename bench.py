@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the RCA delay-and-sum beamformer on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2]
+    python bench.py --impl reference ...          # the reference's CPU arm
+
+Metric: nominal voxel.rx.tx per second (voxels x receive elements x
+transmits, summed over frames) for the Doppler-ensemble workload c2
+(128+128 probe, 11 plane waves, 200 frames of [768 x 128 x 11] I/Q stored
+as FP16, 96 x 96 x 160 voxels, Lanczos a = 4, f-number 1.2), seeded
+synthetic data.  One step = one full beamform of the acquisition: ingest of
+the channel data into the FP16 frame-blocked layout, the window-range
+tables, the fused delay-and-sum kernel over all frames and transmits, and
+the mask.
+
+value     : device-resident inputs, CUDA events on the launching stream.
+e2e       : the same through the C ABI with host (pinned) buffers: the
+            step's H2D copy of the channel data and D2H copy of the volume
+            are inside the timed region.
+roofline  : the fused kernel's FP32 work (active units x (8a + 8) FLOP)
+            over its event-timed duration, against the FP32 FMA peak measured
+            live on this GPU.
+Multi-GPU : each rank beamforms its own ensemble (weak scaling, no
+            data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DAS voxel·rx·tx/s (nominal, summed over frames)"
+UNIT = "voxel·rx·tx/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--storage", default=None, help="float32 | float16 | bfloat16 (default: workload's)")
+    ap.add_argument("--kernel", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--frames-per-block", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-frames", type=int, default=4)
+    ap.add_argument("--cpu-sample-z", type=int, default=8)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(w, data_np, frames: int, zrows: int, kind_pref="reference"):
+    """The reference kernel source on the host cores (oracle/_ref, OpenMP
+    over all cores) on a z-slab x frame sample of the workload; rate in
+    voxel.rx.tx/s.  Falls back to the C restatement ("port")."""
+    import numpy as np
+
+    from oracle import host as H
+    from simu_rca_ab_b200 import workloads as W
+
+    kind = "reference" if (kind_pref == "reference" and H.have_ref_cpu()) else "port"
+    total_units, total_s = 0, 0.0
+    for gi, g in enumerate(w.groups):
+        G = dict(g.Geometry)
+        for k in ("gridBfX", "gridBfY", "gridBfZ"):
+            G[k] = np.asarray(G[k])[:zrows]
+        d = W.as_matlab(W.group_data(w, data_np[:frames], gi))
+        O = {"flagInterpolationLanczos": True, "flagCompounding": True, "flagMaskTransmit": False}
+        r = H.prepare(d, G, g.Transmit, w.Param, O)
+        t = time.perf_counter()
+        if kind == "reference":
+            H.run_ref_cpu(r)
+        else:
+            H.run_c32(r)
+        total_s += time.perf_counter() - t
+        total_units += r.n_pix * r.n_ch * r.n_tx * r.n_frame
+    cores = os.cpu_count()
+    nz, nx, ny = w.grid_shape
+    return {"value": total_units / total_s, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{w.name}: z-slab {zrows} of {nz} depth rows x {nx}x{ny} lateral, all "
+                      f"{w.n_tx} tx x {w.n_ele} rx, {frames} of {w.n_frame} frames; reference 6-tap "
+                      f"'Lanczos 5-lobes' kernel (the reference has no Lanczos-{w.lanczos_a}); "
+                      f"{total_units:.3e} units in {total_s:.1f} s on {cores} threads"}
+
+
+def run_reference(a, rank):
+    """--impl reference: the reference's own kernel source on the host cores."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get(a.workload)
+    frames = max(1, a.cpu_sample_frames)
+    data = W.channel_data(w, seed=0, device="cpu", frames=list(range(frames))).numpy()
+    vals = []
+    for _ in range(a.warmup):
+        cpu_baseline(w, data, 1, 2)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        vals.append(cpu_baseline(w, data, frames, a.cpu_sample_z))
+    el = time.perf_counter() - t0
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * el / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded point scatterers)",
+            "config": {"workload": f"{w.name}: bounded sample per step ({cb['sample']})",
+                       "interp": "reference 6-tap"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        return run_reference(a, rank)
+
+    import ctypes as C
+    import warnings
+
+    import numpy as np
+    import torch
+
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import beamformer as B
+    from simu_rca_ab_b200 import workloads as W
+    from simu_rca_ab_b200.params import normalize
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    w = W.get(a.workload)
+    storage = a.storage or w.storage
+    st_code = {"float32": L.STORE_F32, "float16": L.STORE_F16, "bfloat16": L.STORE_BF16}[storage]
+    kern = L.KERNEL_PLAIN if a.kernel == "plain" else L.KERNEL_FUSED
+
+    data = W.channel_data(w, seed=rank, device=dev)                       # [F][T][E][S] complex64
+    in_dtype = torch.complex32 if storage == "float16" else torch.complex64
+    iq_code = L.IQ_C32 if in_dtype == torch.complex32 else L.IQ_C64
+    eng = B.Engine(dev)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geoms = [eng.geometry(normalize(np.zeros(1, np.complex64), g.Geometry, g.Transmit, w.Param, w.Options))
+                 for g in w.groups]
+    iq_dev = [W.group_data(w, data, gi).contiguous().to(in_dtype) for gi in range(len(w.groups))]
+    F = w.n_frame
+    n_pix = geoms[0].n_pix
+    out = torch.empty((F, 1, n_pix), dtype=torch.complex64, device=dev)
+    mask = torch.empty((1, n_pix), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in w.groups]
+    for ee in evs:
+        for e in ee:
+            e.record(stream)
+    ev_arr = [(C.c_void_p * 5)(*[e.cuda_event for e in ee]) for ee in evs]
+    args = []
+    for gi, g in enumerate(geoms):
+        ar = eng.make_args(g, iq_dev[gi], iq_dtype=iq_code, n_sample=w.n_sample, n_frame=F, out=out, mask=mask,
+                           compound=True, storage=st_code, kernel=kern, accumulate=gi > 0,
+                           frames_per_block=a.frames_per_block)
+        ar.stage_events = C.cast(ev_arr[gi], C.POINTER(C.c_void_p))
+        args.append(ar)
+    ws = [torch.empty(max(256, eng.workspace_bytes(g, ar)), dtype=torch.uint8, device=dev)
+          for g, ar in zip(geoms, args)]
+
+    def step():
+        for g, ar, wsp in zip(geoms, args, ws):
+            eng.run(g, ar, stream=stream, workspace=wsp)
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    peak = C.c_double()
+    L.check(L.lib().rcabf_measure_fp32_peak(C.byref(peak), C.c_void_p(stream.cuda_stream)))
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    n0 = C.c_int64()
+    L.lib().rcabf_take_launch_count(C.byref(n0))
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    t_ev = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
+    t_ev[0].record(stream)
+    for k in range(a.steps):
+        step()
+        t_ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = C.c_int64()
+    L.lib().rcabf_take_launch_count(C.byref(launches))
+    step_ms = [t_ev[k].elapsed_time(t_ev[k + 1]) for k in range(a.steps)]
+    total_ms = t_ev[0].elapsed_time(t_ev[-1])
+    if pg:
+        tt = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        total_ms = tt.item()
+    units = w.units()
+    value = units * world * a.steps / (total_ms * 1e-3)
+
+    # fused-kernel time per launch: stage events of a separate, synchronised step
+    step()
+    torch.cuda.synchronize()
+    fused_ms = sum(ee[2].elapsed_time(ee[3]) for ee in evs)
+    stage_ms = {"ingest": sum(ee[0].elapsed_time(ee[1]) for ee in evs),
+                "ranges": sum(ee[1].elapsed_time(ee[2]) for ee in evs),
+                "das": fused_ms, "mask": sum(ee[3].elapsed_time(ee[4]) for ee in evs)}
+
+    # e2e: host pinned buffers through the C ABI
+    e2e = None
+    if not a.no_e2e:
+        host_in = [t.cpu().pin_memory() for t in iq_dev]
+        host_out = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+        h2d = sum(t.numel() * t.element_size() for t in host_in)
+        d2h = host_out.numel() * host_out.element_size()
+
+        def e2e_step():
+            for t_h, t_d in zip(host_in, iq_dev):
+                t_d.copy_(t_h, non_blocking=True)
+            step()
+            host_out.copy_(out, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if pg:
+            tt = torch.tensor([e2e_ms], device=dev)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            e2e_ms = tt.item()
+        e2e = {"value": units * world * a.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / a.steps}
+
+    line = None
+    if rank == 0:
+        from oracle import host as H
+        # active units (inside aperture and sample window), counted exactly by the oracle
+        active = 0
+        for gi, g in enumerate(w.groups):
+            r = H.prepare(np.zeros((w.n_sample, w.n_ele, 1, g.n_tx), np.complex64), g.Geometry, g.Transmit,
+                          w.Param, {"flagMaskTransmit": False})
+            active += H.active_units(r, H.INTERP_LANCZOS, w.lanczos_a)
+        active *= F
+        fpu = 8 * w.lanczos_a + 8
+        achieved = active * fpu / (fused_ms * 1e-3) / 1e12
+        traffic = None
+        tf = ROOT / "profiles" / f"traffic_{w.name}_{storage}.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value, "traffic": traffic,
+                "peak_source": "FP32 FMA probe kernel timed live in this run (MEASURED_PEAKS.json has no FP32 figure)",
+                "kernel": "fused_das_kernel", "kernel_ms": fused_ms,
+                "work": f"{active:.4e} active units x {fpu} FLOP ({active / (units):.3f} of nominal)",
+                "nominal_achieved": units * fpu / (fused_ms * 1e-3) / 1e12}
+        acc = None
+        if not a.no_accuracy:
+            rng = np.random.default_rng(123)
+            pix = np.sort(rng.choice(n_pix, size=min(2048, n_pix), replace=False))
+            frames = sorted(set([0, F // 2, F - 1]))
+            ref = 0
+            g0 = w.groups[0]
+            for gi, g in enumerate(w.groups):
+                dg = W.group_data(w, data[frames], gi).cpu().numpy()
+                r = H.prepare(W.as_matlab(dg), g.Geometry, g.Transmit, w.Param, {"flagMaskTransmit": False})
+                f64, m64 = H.run_fp64(r, H.INTERP_LANCZOS, w.lanczos_a, data=dg, pix=pix)
+                c64, _ = H.compound(f64, m64, True)
+                ref = ref + c64[:, 0]
+            ours = out[frames][:, 0, :].cpu().numpy()[:, pix]
+            rms, pk = H.error_db(ours, ref)
+            acc = {"rms_db": rms, "peak_db": pk, "vs": "FP64 oracle (complex64 input before storage rounding)",
+                   "sample": f"{pix.size} random voxels x frames {frames}"}
+        cb = None
+        if not a.no_cpu_baseline:
+            dnp = data[: a.cpu_sample_frames].cpu().numpy()
+            cb = cpu_baseline(w, dnp, a.cpu_sample_frames, a.cpu_sample_z)
+        lat = sorted(step_ms)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded point scatterers, -30 dB noise)",
+            "config": {"workload": f"{w.name}: Doppler ensemble, [{w.n_sample} x {w.n_ele} x {w.n_tx} x {F}] I/Q, "
+                                   f"grid {w.grid_shape[1]}x{w.grid_shape[2]}x{w.grid_shape[0]}, Lanczos a={w.lanczos_a}, "
+                                   f"f-number {w.Param['fnumber']}",
+                       "storage": storage, "kernel": a.kernel, "l2": "inputs larger than L2 (no flush needed)",
+                       "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)"},
+            "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
+            "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,240 @@
+/*
+ * rcabf.h -- C ABI of librcabf, a B200 (sm_100a) row-column-array (RCA)
+ * delay-and-sum I/Q beamformer.
+ *
+ * Plain C: pointers, sizes and status codes only.  Device buffers are raw
+ * CUDA device pointers owned by the caller; streams are passed as void*
+ * (a cudaStream_t, NULL = legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   MATLAB/lib/beamformer/RCA/bfVirtualSourceGeneric_RCA.m        the wrapper
+ *   MATLAB/lib/beamformer/RCA/bfVirtualSourceGeneric_RCA.cu:103   the kernel
+ * Each entry point below names the lines it stands in for.
+ */
+#ifndef RCABF_H
+#define RCABF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RCABF_ABI_VERSION 1
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+/* Codes 1..29 correspond one-to-one to the error identifiers raised by the
+ * reference wrapper bfVirtualSourceGeneric_RCA.m (line of the error() call in
+ * brackets).  rcabf_status_string() returns "bfVirtualSourceGeneric_RCA:<id>"
+ * for those, so callers can report the reference identifier. */
+typedef enum rcabf_status {
+    RCABF_OK = 0,
+    RCABF_ERR_DATA_NOT_NUMERIC = 1,            /* :dataNotNumeric [140] */
+    RCABF_ERR_OPTIONS_NOT_STRUCT = 2,          /* :OptionsNotStruct [156] */
+    RCABF_ERR_INTERPOLATION_INVALID = 3,       /* :flagInterpolationLanczosInvalid [168] */
+    RCABF_ERR_COMPOUNDING_INVALID = 4,         /* :flagCompoundingInvalid [177] */
+    RCABF_ERR_MASK_TRANSMIT_INVALID = 5,       /* :flagMaskTransmitInvalid [186] */
+    RCABF_ERR_DECREASE_FACTOR_INVALID = 6,     /* :decreaseFactorGPUInvalid [196] */
+    RCABF_ERR_GRID_MISSING = 7,                /* :gridBfMissing [209] */
+    RCABF_ERR_GRID_INVALID = 8,                /* :gridBfInvalid [223] */
+    RCABF_ERR_POS_ELE_MISSING = 9,             /* :posEleMissing [234] */
+    RCABF_ERR_POS_ELE_INVALID = 10,            /* :posEleInvalid [248] */
+    RCABF_ERR_APERTURE_X_INVALID = 11,         /* :apertureXInvalid [265] */
+    RCABF_ERR_APERTURE_Y_INVALID = 12,         /* :apertureYInvalid [284] */
+    RCABF_ERR_APERTURE_Z_INVALID = 13,         /* :apertureZInvalid [303] */
+    RCABF_ERR_TRANSMIT_NOT_STRUCT = 14,        /* :TransmitNotStruct [313] */
+    RCABF_ERR_THETA_OR_VS_REQUIRED = 15,       /* :ThetaORVirtualSourceRequired [326] */
+    RCABF_ERR_TILTS_NOT_SAME_LENGTH = 16,      /* :tiltsNotSameLength [341] */
+    RCABF_ERR_VS_NOT_SAME_LENGTH = 17,         /* :virtualSourcesNotSameLength [356] */
+    RCABF_ERR_THETA_OR_VS_INVALID = 18,        /* :ThetaORVirtualSourceInvalid [366] */
+    RCABF_ERR_FLAG_RECEIVE_X_INVALID = 19,     /* :flagReceiveXInvalid [378] */
+    RCABF_ERR_PARAM_NOT_STRUCT = 20,           /* :ParamNotStruct [386] */
+    RCABF_ERR_FS_MISSING = 21,                 /* :samplingFrequencyMissing [393] */
+    RCABF_ERR_FS_INVALID = 22,                 /* :samplingFrequencyInvalid [399] */
+    RCABF_ERR_FD_MISSING = 23,                 /* :demodulationFrequencyMissing [406] */
+    RCABF_ERR_FD_INVALID = 24,                 /* :demodulationFrequencyInvalid [412] */
+    RCABF_ERR_SPEED_OF_SOUND_INVALID = 25,     /* :speedOfSoundInvalid [426] */
+    RCABF_ERR_START_TIME_INVALID = 26,         /* :startTimeInvalid [440, 454] */
+    /* Codes of this library (no reference counterpart). */
+    RCABF_ERR_INVALID_ARGUMENT = 100,  /* NULL pointer, bad enum, bad struct_size */
+    RCABF_ERR_SHAPE_MISMATCH = 101,    /* data/output sizes inconsistent with geometry */
+    RCABF_ERR_UNSUPPORTED = 102,       /* valid request this build does not implement */
+    RCABF_ERR_WORKSPACE_TOO_SMALL = 103,
+    RCABF_ERR_OOM_ADMISSION = 104,     /* request larger than the server's HBM budget */
+    RCABF_ERR_TIMEOUT = 105,           /* deadline passed before completion */
+    RCABF_ERR_CUDA = 106,              /* a CUDA runtime call failed */
+    RCABF_ERR_BOUNDS = 107,            /* device-side bound check tripped (never expected) */
+    RCABF_ERR_BAD_HANDLE = 108,
+    RCABF_ERR_CANCELLED = 109,
+    RCABF_ERR_BUSY = 110,              /* server queue full */
+    RCABF_ERR_PENDING = 111            /* poll: request not finished yet */
+} rcabf_status;
+
+const char *rcabf_status_string(int status);
+int rcabf_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Enumerations                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum rcabf_interp {
+    RCABF_INTERP_QUAD3 = 0,   /* reference default, 3-tap quadratic (RCA.cu:355-365) */
+    RCABF_INTERP_REF6 = 1,    /* reference "Lanczos 5-lobes": sinc(x)sinc(x/2), 6 taps (RCA.cu:331-350) */
+    RCABF_INTERP_LANCZOS = 2  /* Lanczos-a: sinc(x)sinc(x/a), 2a taps, a = lanczos_a (2..4) */
+} rcabf_interp;
+
+typedef enum rcabf_table_mode {
+    RCABF_TABLES_EXACT = 0,     /* delays built in FP64 on the host, stored as FP32
+                                   fractional sample indices + unit phasors */
+    RCABF_TABLES_REF_COMPAT = 1 /* reference FP32 arithmetic, operation for operation
+                                   (transmit delay RCA.cu:256-269 with its cancellation) */
+} rcabf_table_mode;
+
+typedef enum rcabf_grid_kind {
+    RCABF_GRID_RECTILINEAR = 0, /* voxel (iz, ix, iy) at (grid_x[ix], grid_y[iy], grid_z[iz]) */
+    RCABF_GRID_POINTS = 1       /* n_pix arbitrary points (grid_x/y/z have n_pix entries) */
+} rcabf_grid_kind;
+
+typedef enum rcabf_iq_dtype {
+    RCABF_IQ_C64 = 0,       /* complex64: float (re, im) pairs */
+    RCABF_IQ_C32 = 1,       /* complex32: half (re, im) pairs */
+    RCABF_IQ_BF16X2 = 2,    /* bfloat16 (re, im) pairs */
+    RCABF_IQ_RF_F32 = 3     /* real float32, I/Q interleaved with Q negated:
+                               IQ(n) = RF(2n) - i*RF(2n+1) (RCA.m:475-477) */
+} rcabf_iq_dtype;
+
+typedef enum rcabf_storage {
+    RCABF_STORE_F32 = 0,   /* complex64 samples in HBM */
+    RCABF_STORE_F16 = 1,   /* half (re, im) in HBM, FP32 arithmetic */
+    RCABF_STORE_BF16 = 2   /* bfloat16 (re, im) in HBM, FP32 arithmetic */
+} rcabf_storage;
+
+typedef enum rcabf_kernel {
+    RCABF_KERNEL_AUTO = 0,  /* fused tiled kernel */
+    RCABF_KERNEL_FUSED = 1, /* persistent voxel-tiled shared-memory gather, all frames in one launch */
+    RCABF_KERNEL_PLAIN = 2  /* one launch per frame, one thread per voxel, global gathers */
+} rcabf_kernel;
+
+/* ------------------------------------------------------------------------ */
+/* Geometry: the probe, the voxel grid, the transmits and the parameters     */
+/* ------------------------------------------------------------------------ */
+/* Fields mirror the reference structs Geometry / Transmit / Param / Options
+ * (bfVirtualSourceGeneric_RCA.m:24-58).  Coordinates in metres, times in
+ * seconds, frequencies in hertz, angles in radians. */
+typedef struct rcabf_geometry_desc {
+    int32_t struct_size;          /* sizeof(rcabf_geometry_desc) */
+    int32_t receive_x;            /* Transmit.flagReceiveX: 1 receive on X (column) elements */
+    /* receive elements, as given: the library centres them (RCA.m:500-502) */
+    int64_t n_ele;
+    const double *pos_ele_x, *pos_ele_y, *pos_ele_z;
+    /* apertures; NaN = element span after centring (RCA.m:505-521) */
+    double aperture_x, aperture_y, aperture_z;
+    /* voxel grid */
+    int32_t grid_kind;            /* rcabf_grid_kind */
+    int32_t reserved0;
+    int64_t n_z, n_x, n_y;        /* RECTILINEAR: axis lengths; POINTS: n_z = n_pix, n_x = n_y = 1 */
+    const double *grid_x, *grid_y, *grid_z; /* axis coordinates or per-point coordinates */
+    int64_t stride_z, stride_x, stride_y;   /* output pixel index = iz*stride_z + ix*stride_x + iy*stride_y */
+    /* transmits: tilt angles (converted to virtual sources 10 m behind the
+       array, RCA.m:527-541) or virtual sources */
+    int64_t n_tx;
+    int32_t use_theta;
+    int32_t reserved1;
+    const double *theta_x, *theta_y;
+    const double *vs_x, *vs_y, *vs_z;
+    /* Param */
+    double fs;                    /* samplingFrequency of the I/Q data */
+    double fd;                    /* demodulationFrequency */
+    double c;                     /* speedOfSound */
+    double t0;                    /* startTime */
+    double fnumber;
+    /* Options */
+    int32_t interp;               /* rcabf_interp */
+    int32_t lanczos_a;            /* RCABF_INTERP_LANCZOS: 2..4 */
+    int32_t table_mode;           /* rcabf_table_mode */
+    int32_t mask_transmit;        /* Options.flagMaskTransmit (RCA.cu:190-219) */
+    /* optional receive aberration law (s), added to the receive delay:
+       per element (Hyp1_save/..._ab_1.cu:306-311) or per (tx, element)
+       (Hyp2/..._ab_2.cu:306-311).  NULL = none. */
+    const double *ab_law;
+    int32_t ab_per_tx;
+    int32_t reserved2;
+} rcabf_geometry_desc;
+
+typedef struct rcabf_geometry rcabf_geometry;
+
+/* Builds the delay/apodisation tables for one probe + grid + transmit set and
+ * keeps them resident on the current device.  Replaces the per-call host
+ * preprocessing of bfVirtualSourceGeneric_RCA.m:459-636 (scalar casts,
+ * centring, apertures, virtual sources and their minimum distance to the
+ * array) and the per-thread delay arithmetic of RCA.cu:255-311.
+ * The stream orders the table uploads; the handle is usable on any stream
+ * of the same device after the stream has reached this point. */
+int rcabf_create_geometry(const rcabf_geometry_desc *desc, void *stream, rcabf_geometry **out);
+int rcabf_destroy_geometry(rcabf_geometry *g);
+
+/* Number of pixels / transmits / receive elements of a geometry. */
+int rcabf_geometry_info(const rcabf_geometry *g, int64_t *n_pix, int64_t *n_tx, int64_t *n_ele);
+
+/* Virtual sources and minimum distance to the array the geometry derived
+ * (RCA.m:527-558), for inspection; arrays of n_tx doubles, any may be NULL. */
+int rcabf_geometry_sources(const rcabf_geometry *g, double *vs_x, double *vs_y, double *vs_z,
+                           double *min_dist);
+
+/* ------------------------------------------------------------------------ */
+/* Beamforming                                                               */
+/* ------------------------------------------------------------------------ */
+typedef struct rcabf_beamform_args {
+    int32_t struct_size;          /* sizeof(rcabf_beamform_args) */
+    int32_t iq_dtype;             /* rcabf_iq_dtype */
+    const void *iq;               /* device: [frame][tx][channel][sample] */
+    int64_t n_sample;             /* I/Q samples per channel (RF_F32: real samples / 2) */
+    int64_t n_ch, n_tx, n_frame;
+    int32_t storage;              /* rcabf_storage */
+    int32_t compound;             /* Options.flagCompounding: 1 sum over transmits */
+    void *out;                    /* device complex64: [frame][compound ? 1 : n_tx][pixel] */
+    float *mask;                  /* device float: [compound ? 1 : n_tx][pixel]; may be NULL */
+    int32_t accumulate;           /* 1: add into out and mask instead of overwriting */
+    int32_t kernel;               /* rcabf_kernel */
+    void *workspace;              /* device scratch, >= rcabf_beamform_workspace_size() */
+    size_t workspace_bytes;
+    int32_t frames_per_block;     /* 0 = automatic */
+    int32_t reserved0;
+    /* NULL, or 5 cudaEvent_t the call records on `stream` before the ingest,
+       after the ingest, after the window-range tables, after the main kernel
+       and after the mask kernel (per-stage device timing) */
+    void *const *stage_events;
+} rcabf_beamform_args;
+
+/* Scratch bytes rcabf_beamform needs for these arguments. */
+int rcabf_beamform_workspace_size(const rcabf_geometry *g, const rcabf_beamform_args *a, size_t *bytes);
+
+/* Beamforms every frame and transmit of one acquisition.  Replaces the
+ * chunked feval/gather loop of bfVirtualSourceGeneric_RCA.m:640-711 and the
+ * kernel bfVirtualSourceGeneric_RCA (RCA.cu:103-390).  Asynchronous on
+ * `stream`; no host synchronisation, no allocation. */
+int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream);
+
+/* Beamforms n independent acquisitions in one persistent launch (all must
+ * share interp, storage and frames_per_block). */
+int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beamform_args *a,
+                         void *stream);
+
+/* Count of device-side bound-check trips since the last call (expected 0). */
+int rcabf_take_error_count(int64_t *count);
+
+/* Number of kernel launches this library issued since the last call. */
+int rcabf_take_launch_count(int64_t *count);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s), from a probe
+ * kernel of independent FMA chains; the denominator of the beamformer's
+ * FP32 roofline.  Synchronises the stream. */
+int rcabf_measure_fp32_peak(double *tflops, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RCABF_H */

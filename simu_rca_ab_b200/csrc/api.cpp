@@ -1,0 +1,438 @@
+// C ABI of librcabf (include/rcabf.h): geometry handles, launch planning and
+// the beamform entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/rcabf.h"
+#include "geometry.h"
+#include "launchers.h"
+#include "plan.h"
+
+using namespace rcabf;
+
+namespace rcabf {
+
+std::atomic<int64_t> g_launches{0};
+
+struct DeviceState {
+    unsigned long long *err = nullptr;
+    int n_sm = 0;
+    std::mutex mu;
+    std::map<std::array<int64_t, 5>, int> occ;   // (mode, kind, fb, store, smem) -> CTAs/SM
+    std::map<std::array<int64_t, 5>, bool> prepared;
+};
+
+static std::mutex g_dev_mu;
+static std::map<int, DeviceState *> g_dev;
+
+DeviceState *device_state(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    auto it = g_dev.find(dev);
+    if (it != g_dev.end()) return it->second;
+    DeviceState *s = new DeviceState();
+    cudaDeviceGetAttribute(&s->n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaMalloc(&s->err, sizeof(unsigned long long)) != cudaSuccess) s->err = nullptr;
+    else cudaMemset(s->err, 0, sizeof(unsigned long long));
+    g_dev[dev] = s;
+    return s;
+}
+
+static int pow2_ceil(int64_t x)
+{
+    int p = 1;
+    while (p < x && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+TileShape default_tile(const rcabf_geometry *g)
+{
+    // Lanes of a warp cover a (u, v) patch at one depth: receive and transmit
+    // delays differ little across it, so the taps of a warp fall on few rows
+    // of the shared-memory window.  Warps stack along z.
+    int tu = std::min(4, pow2_ceil(g->n_u));
+    int tv = std::min(8, pow2_ceil(g->n_v));
+    if (tu * tv < 32 && g->n_u > tu) tu = std::min(32 / tv, pow2_ceil(g->n_u));
+    const int tz = FUSED_THREADS / (tu * tv);
+    return TileShape{tu, tv, tz};
+}
+
+int choose_fb(int64_t n_frame, int requested)
+{
+    if (requested > 0) return requested;
+    if (n_frame >= 8) return 8;
+    return pow2_ceil(n_frame);
+}
+
+int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
+{
+    if (!g || !a) return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->struct_size != (int32_t)sizeof(rcabf_beamform_args)) return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->n_sample < 1 || a->n_frame < 1) return RCABF_ERR_SHAPE_MISMATCH;
+    if (a->n_ch != g->n_ele || a->n_tx != g->n_tx) return RCABF_ERR_SHAPE_MISMATCH;
+    if (a->n_sample > (1 << 24) || a->n_frame > (1 << 24)) return RCABF_ERR_UNSUPPORTED;
+    if (a->iq_dtype < RCABF_IQ_C64 || a->iq_dtype > RCABF_IQ_RF_F32) return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->storage < RCABF_STORE_F32 || a->storage > RCABF_STORE_BF16) return RCABF_ERR_INVALID_ARGUMENT;
+    if (g->mode == MODE_REF && a->storage != RCABF_STORE_F32) return RCABF_ERR_UNSUPPORTED;
+    const int fb_req = a->frames_per_block;
+    if (fb_req != 0 && fb_req != 1 && fb_req != 2 && fb_req != 4 && fb_req != 8 && fb_req != 16)
+        return RCABF_ERR_INVALID_ARGUMENT;
+    p = Plan{};
+    p.kernel = (a->kernel == RCABF_KERNEL_PLAIN) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
+    if (p.kernel == RCABF_KERNEL_PLAIN) {
+        p.total = 0;
+        return RCABF_OK;
+    }
+    p.store = a->storage;
+    p.fb = choose_fb(a->n_frame, fb_req);
+    p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
+    p.ts = default_tile(g);
+    p.tiles_z = (int)((g->n_z + p.ts.tz - 1) / p.ts.tz);
+    p.tiles_u = (int)((g->n_u + p.ts.tu - 1) / p.ts.tu);
+    p.tiles_v = (int)((g->n_v + p.ts.tv - 1) / p.ts.tv);
+    const int es = store_bytes(p.store);
+    const int rowb = p.fb * es;
+    p.row_words = rowb >= 16 ? (rowb + 16) / 4 : rowb / 4;
+    const int want = g->window_rows(p.ts);
+    const int cap = (int)(SMEM_BUDGET / (FUSED_STAGES * p.row_words * 4));
+    p.wmax = std::max(kind_taps(g->kind), std::min(want, cap));
+    p.smem = (size_t)FUSED_STAGES * p.wmax * p.row_words * 4;
+    p.slab_bytes = ((int64_t)a->n_sample * rowb + 15) / 16 * 16;
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    size_t off = 0;
+    p.off_S = off;
+    off += al((size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes);
+    p.off_rxr = off;
+    off += al((size_t)g->n_ele * p.tiles_u * p.tiles_z * sizeof(float2));
+    p.off_txr = off;
+    off += al((size_t)g->n_tx * p.tiles_v * p.tiles_z * sizeof(float2));
+    p.total = off;
+    p.n_items = (int64_t)p.n_fb * p.tiles_z * p.tiles_u * p.tiles_v;
+    return RCABF_OK;
+}
+
+static void mark(const rcabf_beamform_args *a, int i, cudaStream_t st)
+{
+    if (a->stage_events && a->stage_events[i]) cudaEventRecord((cudaEvent_t)a->stage_events[i], st);
+}
+
+// Fills the per-job descriptor and launches the job's ingest and range kernels.
+int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, FusedJob &J, cudaStream_t st,
+              const rcabf_beamform_args *marks = nullptr)
+{
+    char *ws = reinterpret_cast<char *>(a->workspace);
+    IngestParams ip{};
+    ip.iq = a->iq; ip.iq_dtype = a->iq_dtype; ip.n_sample = (int)a->n_sample; ip.n_ele = g->n_ele;
+    ip.n_tx = g->n_tx; ip.n_frame = a->n_frame; ip.fb = p.fb; ip.n_fb = p.n_fb;
+    ip.S = ws + p.off_S; ip.slab_bytes = p.slab_bytes;
+    if (launch_ingest(ip, p.store, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    if (marks) mark(marks, 1, st);
+    RangeParams rr{};
+    rr.tab = g->rx_tab; rr.out = reinterpret_cast<float2 *>(ws + p.off_rxr); rr.rows = g->n_ele;
+    rr.n_a = g->n_u; rr.n_z = g->n_z; rr.ta = p.ts.tu; rr.tz = p.ts.tz; rr.tiles_a = p.tiles_u;
+    rr.tiles_z = p.tiles_z; rr.mode = g->mode; rr.is_rx = 1;
+    if (launch_range(rr, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    RangeParams tr = rr;
+    tr.tab = g->tx_tab; tr.out = reinterpret_cast<float2 *>(ws + p.off_txr); tr.rows = g->n_tx;
+    tr.n_a = g->n_v; tr.ta = p.ts.tv; tr.tiles_a = p.tiles_v; tr.is_rx = 0;
+    if (launch_range(tr, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    g_launches += 3;
+    if (marks) mark(marks, 2, st);
+
+    J = FusedJob{};
+    J.g = g->dev();
+    J.S = ws + p.off_S;
+    J.slab_bytes = p.slab_bytes;
+    J.rx_range = reinterpret_cast<const float2 *>(ws + p.off_rxr);
+    J.tx_range = reinterpret_cast<const float2 *>(ws + p.off_txr);
+    J.out = reinterpret_cast<float2 *>(a->out);
+    J.n_fb = p.n_fb; J.n_frame = (int)a->n_frame; J.n_sample = (int)a->n_sample;
+    J.compound = a->compound ? 1 : 0; J.accumulate = a->accumulate ? 1 : 0;
+    J.tiles_z = p.tiles_z; J.tiles_u = p.tiles_u; J.tiles_v = p.tiles_v;
+    J.tu = p.ts.tu; J.tv = p.ts.tv; J.tz = p.ts.tz;
+    return RCABF_OK;
+}
+
+int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaStream_t st)
+{
+    DeviceState *ds = device_state(g0->device);
+    prm.err_count = ds->err;
+    const std::array<int64_t, 5> key{g0->mode, g0->kind, p.fb, p.store, (int64_t)prm.wmax * prm.row_words * 4};
+    const size_t smem = (size_t)key[4];
+    int occ;
+    {
+        std::lock_guard<std::mutex> lk(ds->mu);
+        if (!ds->prepared[key]) {
+            if (prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem) != cudaSuccess) return RCABF_ERR_CUDA;
+            ds->prepared[key] = true;
+            ds->occ[key] = fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
+        }
+        occ = std::max(1, ds->occ[key]);
+    }
+    const int64_t grid = std::min<int64_t>(prm.n_items, (int64_t)ds->n_sm * occ);
+    if (grid <= 0) return RCABF_OK;
+    if (launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st) != cudaSuccess)
+        return RCABF_ERR_CUDA;
+    g_launches += 1;
+    return RCABF_OK;
+}
+
+static int check_ptrs(const rcabf_beamform_args *a, const Plan &p)
+{
+    if (!a->iq || !a->out) return RCABF_ERR_INVALID_ARGUMENT;
+    if (p.kernel == RCABF_KERNEL_FUSED) {
+        if (a->workspace_bytes < p.total || (p.total && !a->workspace)) return RCABF_ERR_WORKSPACE_TOO_SMALL;
+        if (((uintptr_t)a->workspace) % 256) return RCABF_ERR_INVALID_ARGUMENT;
+    }
+    if (((uintptr_t)a->out) % 8) return RCABF_ERR_INVALID_ARGUMENT;
+    return RCABF_OK;
+}
+
+int beamform_one(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t st)
+{
+    Plan p;
+    int s = plan_beamform(g, a, p);
+    if (s != RCABF_OK) return s;
+    if ((s = check_ptrs(a, p)) != RCABF_OK) return s;
+    device_state(g->device);
+    mark(a, 0, st);
+    if (p.kernel == RCABF_KERNEL_PLAIN) {
+        mark(a, 1, st);
+        mark(a, 2, st);
+        PlainParams pp{};
+        pp.g = g->dev(); pp.iq = a->iq; pp.iq_dtype = a->iq_dtype; pp.n_sample = (int)a->n_sample;
+        pp.n_frame = a->n_frame; pp.compound = a->compound ? 1 : 0; pp.accumulate = a->accumulate ? 1 : 0;
+        pp.out = reinterpret_cast<float2 *>(a->out);
+        pp.err_count = device_state(g->device)->err;
+        for (int64_t f = 0; f < a->n_frame; ++f) {
+            pp.frame = f;
+            if (launch_plain(g->mode, g->kind, pp, st) != cudaSuccess) return RCABF_ERR_CUDA;
+            g_launches += 1;
+        }
+    } else {
+        FusedParams prm{};
+        if ((s = stage_job(g, a, p, prm.jobs[0], st, a)) != RCABF_OK) return s;
+        prm.jobs[0].item_begin = 0;
+        prm.n_jobs = 1;
+        prm.wmax = p.wmax;
+        prm.row_words = p.row_words;
+        prm.n_items = p.n_items;
+        if ((s = launch_fused_jobs(g, prm, p, st)) != RCABF_OK) return s;
+    }
+    mark(a, 3, st);
+    if (a->mask) {
+        if (launch_mask(g->dev(), a->mask, a->compound ? 1 : 0, a->accumulate ? 1 : 0, st) != cudaSuccess)
+            return RCABF_ERR_CUDA;
+        g_launches += 1;
+    }
+    mark(a, 4, st);
+    return RCABF_OK;
+}
+
+}  // namespace rcabf
+
+// --------------------------------------------------------------------------
+// C ABI
+// --------------------------------------------------------------------------
+extern "C" {
+
+const char *rcabf_status_string(int s)
+{
+    switch (s) {
+    case RCABF_OK: return "ok";
+    case RCABF_ERR_DATA_NOT_NUMERIC: return "bfVirtualSourceGeneric_RCA:dataNotNumeric";
+    case RCABF_ERR_OPTIONS_NOT_STRUCT: return "bfVirtualSourceGeneric_RCA:OptionsNotStruct";
+    case RCABF_ERR_INTERPOLATION_INVALID: return "bfVirtualSourceGeneric_RCA:flagInterpolationLanczosInvalid";
+    case RCABF_ERR_COMPOUNDING_INVALID: return "bfVirtualSourceGeneric_RCA:flagCompoundingInvalid";
+    case RCABF_ERR_MASK_TRANSMIT_INVALID: return "bfVirtualSourceGeneric_RCA:flagMaskTransmitInvalid";
+    case RCABF_ERR_DECREASE_FACTOR_INVALID: return "bfVirtualSourceGeneric_RCA:decreaseFactorGPUInvalid";
+    case RCABF_ERR_GRID_MISSING: return "bfVirtualSourceGeneric_RCA:gridBfMissing";
+    case RCABF_ERR_GRID_INVALID: return "bfVirtualSourceGeneric_RCA:gridBfInvalid";
+    case RCABF_ERR_POS_ELE_MISSING: return "bfVirtualSourceGeneric_RCA:posEleMissing";
+    case RCABF_ERR_POS_ELE_INVALID: return "bfVirtualSourceGeneric_RCA:posEleInvalid";
+    case RCABF_ERR_APERTURE_X_INVALID: return "bfVirtualSourceGeneric_RCA:apertureXInvalid";
+    case RCABF_ERR_APERTURE_Y_INVALID: return "bfVirtualSourceGeneric_RCA:apertureYInvalid";
+    case RCABF_ERR_APERTURE_Z_INVALID: return "bfVirtualSourceGeneric_RCA:apertureZInvalid";
+    case RCABF_ERR_TRANSMIT_NOT_STRUCT: return "bfVirtualSourceGeneric_RCA:TransmitNotStruct";
+    case RCABF_ERR_THETA_OR_VS_REQUIRED: return "bfVirtualSourceGeneric_RCA:ThetaORVirtualSourceRequired";
+    case RCABF_ERR_TILTS_NOT_SAME_LENGTH: return "bfVirtualSourceGeneric_RCA:tiltsNotSameLength";
+    case RCABF_ERR_VS_NOT_SAME_LENGTH: return "bfVirtualSourceGeneric_RCA:virtualSourcesNotSameLength";
+    case RCABF_ERR_THETA_OR_VS_INVALID: return "bfVirtualSourceGeneric_RCA:ThetaORVirtualSourceInvalid";
+    case RCABF_ERR_FLAG_RECEIVE_X_INVALID: return "bfVirtualSourceGeneric_RCA:flagReceiveXInvalid";
+    case RCABF_ERR_PARAM_NOT_STRUCT: return "bfVirtualSourceGeneric_RCA:ParamNotStruct";
+    case RCABF_ERR_FS_MISSING: return "bfVirtualSourceGeneric_RCA:samplingFrequencyMissing";
+    case RCABF_ERR_FS_INVALID: return "bfVirtualSourceGeneric_RCA:samplingFrequencyInvalid";
+    case RCABF_ERR_FD_MISSING: return "bfVirtualSourceGeneric_RCA:demodulationFrequencyMissing";
+    case RCABF_ERR_FD_INVALID: return "bfVirtualSourceGeneric_RCA:demodulationFrequencyInvalid";
+    case RCABF_ERR_SPEED_OF_SOUND_INVALID: return "bfVirtualSourceGeneric_RCA:speedOfSoundInvalid";
+    case RCABF_ERR_START_TIME_INVALID: return "bfVirtualSourceGeneric_RCA:startTimeInvalid";
+    case RCABF_ERR_INVALID_ARGUMENT: return "rcabf:invalidArgument";
+    case RCABF_ERR_SHAPE_MISMATCH: return "rcabf:shapeMismatch";
+    case RCABF_ERR_UNSUPPORTED: return "rcabf:unsupported";
+    case RCABF_ERR_WORKSPACE_TOO_SMALL: return "rcabf:workspaceTooSmall";
+    case RCABF_ERR_OOM_ADMISSION: return "rcabf:oomAdmission";
+    case RCABF_ERR_TIMEOUT: return "rcabf:timeout";
+    case RCABF_ERR_CUDA: return "rcabf:cudaError";
+    case RCABF_ERR_BOUNDS: return "rcabf:boundsCheck";
+    case RCABF_ERR_BAD_HANDLE: return "rcabf:badHandle";
+    case RCABF_ERR_CANCELLED: return "rcabf:cancelled";
+    case RCABF_ERR_BUSY: return "rcabf:busy";
+    case RCABF_ERR_PENDING: return "rcabf:pending";
+    default: return "rcabf:unknown";
+    }
+}
+
+int rcabf_abi_version(void) { return RCABF_ABI_VERSION; }
+
+int rcabf_create_geometry(const rcabf_geometry_desc *desc, void *stream, rcabf_geometry **out)
+{
+    int s = build_geometry(desc, (cudaStream_t)stream, out);
+    if (s == RCABF_OK) device_state((*out)->device);
+    return s;
+}
+
+int rcabf_destroy_geometry(rcabf_geometry *g)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    free_geometry(g);
+    return RCABF_OK;
+}
+
+int rcabf_geometry_info(const rcabf_geometry *g, int64_t *n_pix, int64_t *n_tx, int64_t *n_ele)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    if (n_pix) *n_pix = g->n_pix;
+    if (n_tx) *n_tx = g->n_tx;
+    if (n_ele) *n_ele = g->n_ele;
+    return RCABF_OK;
+}
+
+int rcabf_geometry_sources(const rcabf_geometry *g, double *vs_x, double *vs_y, double *vs_z, double *min_dist)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    for (int t = 0; t < g->n_tx; ++t) {
+        if (vs_x) vs_x[t] = g->vs_x[t];
+        if (vs_y) vs_y[t] = g->vs_y[t];
+        if (vs_z) vs_z[t] = g->vs_z[t];
+        if (min_dist) min_dist[t] = g->min_dist[t];
+    }
+    return RCABF_OK;
+}
+
+int rcabf_beamform_workspace_size(const rcabf_geometry *g, const rcabf_beamform_args *a, size_t *bytes)
+{
+    if (!bytes) return RCABF_ERR_INVALID_ARGUMENT;
+    Plan p;
+    int s = plan_beamform(const_cast<rcabf_geometry *>(g), a, p);
+    if (s == RCABF_OK) *bytes = p.total;
+    return s;
+}
+
+int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    return beamform_one(const_cast<rcabf_geometry *>(g), a, (cudaStream_t)stream);
+}
+
+int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_beamform_args *as, void *stream)
+{
+    if (n < 1 || n > MAX_JOBS || !gs || !as) return RCABF_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    rcabf_geometry *g0 = const_cast<rcabf_geometry *>(gs[0]);
+    if (!g0) return RCABF_ERR_BAD_HANDLE;
+    FusedParams prm{};
+    Plan p0;
+    int64_t items = 0;
+    int wmax = 0;
+    for (int i = 0; i < n; ++i) {
+        rcabf_geometry *g = const_cast<rcabf_geometry *>(gs[i]);
+        if (!g) return RCABF_ERR_BAD_HANDLE;
+        if (as[i].frames_per_block <= 0 || as[i].frames_per_block != as[0].frames_per_block)
+            return RCABF_ERR_INVALID_ARGUMENT;
+        if (as[i].kernel == RCABF_KERNEL_PLAIN) return RCABF_ERR_INVALID_ARGUMENT;
+        if (g->mode != g0->mode || g->kind != g0->kind || g->device != g0->device ||
+            as[i].storage != as[0].storage)
+            return RCABF_ERR_UNSUPPORTED;
+        Plan p;
+        int s = plan_beamform(g, &as[i], p);
+        if (s != RCABF_OK) return s;
+        if ((s = check_ptrs(&as[i], p)) != RCABF_OK) return s;
+        if (i == 0) p0 = p;
+        wmax = std::max(wmax, p.wmax);
+        if ((s = stage_job(g, &as[i], p, prm.jobs[i], st)) != RCABF_OK) return s;
+        prm.jobs[i].item_begin = items;
+        items += p.n_items;
+    }
+    prm.n_jobs = n;
+    prm.wmax = wmax;
+    prm.row_words = p0.row_words;
+    prm.n_items = items;
+    int s = launch_fused_jobs(g0, prm, p0, st);
+    if (s != RCABF_OK) return s;
+    for (int i = 0; i < n; ++i) {
+        if (!as[i].mask) continue;
+        if (launch_mask(gs[i]->dev(), as[i].mask, as[i].compound ? 1 : 0, as[i].accumulate ? 1 : 0, st) !=
+            cudaSuccess)
+            return RCABF_ERR_CUDA;
+        g_launches += 1;
+    }
+    return RCABF_OK;
+}
+
+int rcabf_take_error_count(int64_t *count)
+{
+    if (!count) return RCABF_ERR_INVALID_ARGUMENT;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DeviceState *ds = device_state(dev);
+    unsigned long long h = 0;
+    if (!ds->err) return RCABF_ERR_CUDA;
+    if (cudaMemcpy(&h, ds->err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return RCABF_ERR_CUDA;
+    if (cudaMemset(ds->err, 0, sizeof(h)) != cudaSuccess) return RCABF_ERR_CUDA;
+    *count = (int64_t)h;
+    return RCABF_OK;
+}
+
+int rcabf_take_launch_count(int64_t *count)
+{
+    if (!count) return RCABF_ERR_INVALID_ARGUMENT;
+    *count = g_launches.exchange(0);
+    return RCABF_OK;
+}
+
+int rcabf_measure_fp32_peak(double *tflops, void *stream)
+{
+    if (!tflops) return RCABF_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DeviceState *ds = device_state(dev);
+    float *out = nullptr;
+    if (cudaMalloc(&out, 256 * sizeof(float)) != cudaSuccess) return RCABF_ERR_CUDA;
+    const int blocks = ds->n_sm * 8, iters = 4096;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    launch_fma_probe(out, blocks, 64, st);  // warm-up
+    cudaEventRecord(e0, st);
+    launch_fma_probe(out, blocks, iters, st);
+    cudaEventRecord(e1, st);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (ce != cudaSuccess || ms <= 0.f) return RCABF_ERR_CUDA;
+    const double flops = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return RCABF_OK;
+}
+
+}  // extern "C"

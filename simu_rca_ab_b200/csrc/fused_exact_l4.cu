@@ -1,0 +1,3 @@
+// Fused + plain kernel instantiations: EXACT tables, kind K_LANCZOS4.
+#include "fused_inst.cuh"
+RCABF_EXACT_TU(K_LANCZOS4, exact_l4)

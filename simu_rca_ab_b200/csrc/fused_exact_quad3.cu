@@ -1,0 +1,3 @@
+// Fused + plain kernel instantiations: EXACT tables, kind K_QUAD3.
+#include "fused_inst.cuh"
+RCABF_EXACT_TU(K_QUAD3, exact_quad3)

@@ -1,0 +1,3 @@
+// Fused + plain kernel instantiations: EXACT tables, kind K_REF6.
+#include "fused_inst.cuh"
+RCABF_EXACT_TU(K_REF6, exact_ref6)

@@ -1,0 +1,76 @@
+// Explicit instantiation helpers for the fused and plain kernels.  Each
+// instantiation translation unit includes this header and defines one entry
+// point for one (mode, kind), so the many template variants compile in
+// parallel.
+#pragma once
+
+#include "das_kernels.cuh"
+#include "launchers.h"
+
+namespace rcabf {
+
+// what: 0 launch, 1 set the shared-memory attribute, 2 query occupancy.
+template <int MODE, int KIND, int FB, int STORE>
+static cudaError_t fused_do(const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
+{
+    auto k = fused_das_kernel<MODE, KIND, FB, STORE>;
+    if (what == 1) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (what == 2) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, FUSED_THREADS, smem);
+    k<<<grid, FUSED_THREADS, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+template <int MODE, int KIND, int STORE>
+static cudaError_t fused_fb(int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
+{
+    switch (fb) {
+    case 1: return fused_do<MODE, KIND, 1, STORE>(p, grid, smem, st, what, occ);
+    case 2: return fused_do<MODE, KIND, 2, STORE>(p, grid, smem, st, what, occ);
+    case 4: return fused_do<MODE, KIND, 4, STORE>(p, grid, smem, st, what, occ);
+    case 8: return fused_do<MODE, KIND, 8, STORE>(p, grid, smem, st, what, occ);
+    case 16: return fused_do<MODE, KIND, 16, STORE>(p, grid, smem, st, what, occ);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int MODE, int KIND, int IQ>
+static cudaError_t plain_do(const PlainParams &p, cudaStream_t st)
+{
+    const int64_t n = p.g.n_z * p.g.n_u * p.g.n_v;
+    plain_das_kernel<MODE, KIND, IQ><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <int MODE, int KIND>
+static cudaError_t plain_iq(const PlainParams &p, cudaStream_t st)
+{
+    switch (p.iq_dtype) {
+    case 0: return plain_do<MODE, KIND, 0>(p, st);
+    case 1: return plain_do<MODE, KIND, 1>(p, st);
+    case 2: return plain_do<MODE, KIND, 2>(p, st);
+    case 3: return plain_do<MODE, KIND, 3>(p, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace rcabf
+
+// Defines rcabf::fused_entry_<NAME>(store, fb, ...) for all three storage
+// types and rcabf::plain_entry_<NAME>(...).
+#define RCABF_EXACT_TU(KIND, NAME)                                                                  \
+    namespace rcabf {                                                                               \
+    cudaError_t fused_entry_##NAME(int store, int fb, const FusedParams *p, int grid, size_t smem,  \
+                                   cudaStream_t st, int what, int *occ)                             \
+    {                                                                                               \
+        switch (store) {                                                                            \
+        case ST_F32: return fused_fb<MODE_EXACT, KIND, ST_F32>(fb, p, grid, smem, st, what, occ);   \
+        case ST_F16: return fused_fb<MODE_EXACT, KIND, ST_F16>(fb, p, grid, smem, st, what, occ);   \
+        case ST_BF16: return fused_fb<MODE_EXACT, KIND, ST_BF16>(fb, p, grid, smem, st, what, occ); \
+        default: return cudaErrorInvalidValue;                                                      \
+        }                                                                                           \
+    }                                                                                               \
+    cudaError_t plain_entry_##NAME(const PlainParams &p, cudaStream_t st)                           \
+    {                                                                                               \
+        return plain_iq<MODE_EXACT, KIND>(p, st);                                                   \
+    }                                                                                               \
+    }

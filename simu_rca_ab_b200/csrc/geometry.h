@@ -1,0 +1,76 @@
+// Host-side geometry object of librcabf: validated acquisition description,
+// the derived virtual sources, and the device-resident delay tables.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rcabf.h"
+#include "rcabf_internal.h"
+
+namespace rcabf {
+
+struct TileShape {
+    int tu, tv, tz;
+    bool operator<(const TileShape &o) const
+    {
+        return std::array<int, 3>{tu, tv, tz} < std::array<int, 3>{o.tu, o.tv, o.tz};
+    }
+};
+
+// Spread of the table delay inside the tiles of one shape, used to size the
+// shared-memory window (see window_rows()).
+struct TileSpread {
+    std::vector<float> tx_spread;  // per tile-z: max over (tx, tile-v) of max-min
+    std::vector<float> rx_spread;  // per tile-z: max over (ele, tile-u) of max-min
+};
+
+}  // namespace rcabf
+
+struct rcabf_geometry {
+    int device = 0;
+    int mode = 0;          // rcabf::Mode
+    int interp = 0, lanczos_a = 0, kind = 0;
+    int receive_x = 1, mask_transmit = 0;
+    int grid_kind = 0;
+    int64_t n_z = 0, n_u = 0, n_v = 0, s_z = 0, s_u = 0, s_v = 0, n_pix = 0;
+    int n_ele = 0, n_tx = 0;
+    double fs = 0, fd = 0, c = 0, t0 = 0, fnumber = 0;
+    double ap_x = 0, ap_y = 0, ap_z = 0;
+    std::vector<double> vs_x, vs_y, vs_z, min_dist;
+    int has_ab = 0, ab_per_tx = 0;
+
+    // host copies of the table delays (x component) for window sizing
+    std::vector<float> rx_delay;   // [n_ele][n_rxkey], NaN where invalid
+    std::vector<float> tx_delay;   // [n_tx][n_txkey]
+    std::vector<float> ab_host;    // [n_ele] or [n_tx][n_ele] in table units
+
+    // device buffers (owned)
+    float4 *rx_tab = nullptr;
+    float4 *tx_tab = nullptr;
+    uint8_t *cone_u = nullptr;
+    float *apod_sum = nullptr;
+    float *ab = nullptr;
+    float2 *ab_ph = nullptr;
+    rcabf::RefScalars ref{};
+
+    std::mutex mu;
+    std::map<rcabf::TileShape, rcabf::TileSpread> spreads;
+
+    rcabf::DevGeom dev() const;
+    // Upper bound of the window rows any tile of this shape needs for one
+    // (tx, ele) step: spread of the transmit delay + spread of the receive
+    // delay inside the tile (in samples) + the taps + rounding slack.
+    int window_rows(const rcabf::TileShape &ts);
+};
+
+namespace rcabf {
+int build_geometry(const rcabf_geometry_desc *d, cudaStream_t st, rcabf_geometry **out);
+void free_geometry(rcabf_geometry *g);
+}  // namespace rcabf

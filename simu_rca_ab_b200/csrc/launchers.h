@@ -1,0 +1,67 @@
+// Host-side launch entry points of the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "rcabf_internal.h"
+
+namespace rcabf {
+
+struct IngestParams {
+    const void *iq;
+    int32_t iq_dtype;
+    int32_t n_sample, n_ele, n_tx;
+    int64_t n_frame;
+    int32_t fb, n_fb;
+    void *S;
+    int64_t slab_bytes;
+};
+
+struct RangeParams {
+    const float4 *tab;
+    float2 *out;
+    int64_t rows, n_a, n_z;
+    int32_t ta, tz, tiles_a, tiles_z;
+    int32_t mode, is_rx;
+};
+
+// Inputs of the REF_COMPAT table kernels: single-precision copies of what the
+// reference wrapper hands its kernel (RCA.m:601-626), per table key.
+struct RefTableParams {
+    float4 *rx_tab;        // [n_ele][n_rxkey]
+    float4 *tx_tab;        // [n_tx][n_txkey]
+    uint8_t *cone_u;       // [n_tx][n_rxkey] or NULL
+    float *apod_sum;       // [n_rxkey]
+    const float *rx_key_u, *rx_key_z;   // per rx key
+    const float *tx_key_v, *tx_key_z;   // per tx key
+    const float *ele_u, *ele_z;         // per element (receive axis, depth)
+    const float *vs_u, *vs_v, *vs_z;    // per tx, virtual source along u, v, z
+    const float *min_dist;              // per tx
+    int64_t n_rxkey, n_txkey;
+    int32_t n_ele, n_tx;
+    float half_ap_u, half_ap_v, ap_z;   // half apertures along u / v, aperture along z
+    float fnumber, inv_c;
+    int32_t receive_x;
+    int32_t mask_transmit;
+    float fd, fs;          // for the phase-rate ratio fdividef(fd, fs) (RCA.cu:372)
+    float *ratio_out;      // one float
+};
+
+cudaError_t launch_ingest(const IngestParams &p, int store, cudaStream_t st);
+cudaError_t launch_range(const RangeParams &p, cudaStream_t st);
+cudaError_t launch_mask(const DevGeom &g, float *mask, int compound, int accumulate, cudaStream_t st);
+cudaError_t launch_fma_probe(float *out, int blocks, int iters, cudaStream_t st);
+cudaError_t launch_ref_tables(const RefTableParams &p, cudaStream_t st);
+
+// Fused kernel (persistent).  kind: Kind, store: Store, fb in {1,2,4,8,16}.
+cudaError_t launch_fused(int mode, int kind, int fb, int store, const FusedParams &p, int grid,
+                         size_t smem, cudaStream_t st);
+// Shared memory the fused kernel may use (opt-in beyond 48 KB), per variant.
+cudaError_t prepare_fused(int mode, int kind, int fb, int store, size_t smem);
+// Resident CTAs per SM for a variant at a given dynamic shared memory size.
+int fused_occupancy(int mode, int kind, int fb, int store, size_t smem);
+
+// Plain kernel: one frame.
+cudaError_t launch_plain(int mode, int kind, const PlainParams &p, cudaStream_t st);
+
+}  // namespace rcabf

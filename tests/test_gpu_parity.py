@@ -1,0 +1,210 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+* REF_COMPAT tables + the reference's interpolation kernels: against the
+  reference kernel source compiled for sm_100a without fast math or FMA
+  contraction (oracle/_ref/librca_ref_gpu_strict.so), tolerance 1e-4
+  relative RMS (expected: identical bits).
+* EXACT tables: against the FP64 oracle, tolerance -60 dB RMS for FP32 and
+  FP16 storage (BF16 storage: -45 dB, its 8-bit mantissa).
+* Internal consistency: fused vs plain kernel, frame-block sizes, batch vs
+  single launches, per-transmit vs compounded, both receive orientations,
+  point-list grids, the transmit-cone mask, real (interleaved RF) input.
+"""
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import host as H
+from tests.golden.make_golden import CASES, case, load
+
+pytestmark = pytest.mark.gpu
+
+REF_TOL = 1e-4          # relative RMS, REF_COMPAT vs reference kernel
+DB_FP32 = -60.0         # dB RMS vs FP64 oracle
+DB_FP16 = -60.0
+DB_BF16 = -45.0
+
+
+@pytest.fixture(scope="module")
+def bf(cuda):
+    from simu_rca_ab_b200 import beamformer as B
+    return B
+
+
+def run(bf, data, G, T, P, O, **opts):
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        return bf.bf_rca(data, G, T, P, {**O, **opts})
+
+
+def _errcount():
+    import ctypes as C
+    from simu_rca_ab_b200 import _lib as L
+    n = C.c_int64()
+    L.check(L.lib().rcabf_take_error_count(C.byref(n)))
+    return n.value
+
+
+# --------------------------------------------------------------------------
+# REF_COMPAT vs the reference kernel on the GPU
+# --------------------------------------------------------------------------
+@pytest.mark.skipif(not H.have_ref_gpu("strict"), reason="oracle/_ref GPU build missing")
+@pytest.mark.parametrize("kernel", ["fused", "plain"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_ref_compat_matches_reference_kernel(bf, name, kernel):
+    data, G, T, P, O, outs = load(name)
+    r = H.prepare(data, G, T, P, O)
+    o2, m2 = H.run_ref_gpu(r, "strict")
+    c2, mc2 = H.compound(o2, m2, True)
+    db_ref, mk_ref = H.matlab_shape(r, c2, mc2)
+    db, mk = run(bf, data, G, T, P, O, tableMode="ref_compat", kernel=kernel)
+    assert db.shape == db_ref.shape and mk.shape == mk_ref.shape
+    err = H.rel_rms(db, db_ref)
+    print(f"{name} {kernel}: rel RMS vs reference GPU kernel {err:.3e}, "
+          f"identical bits {np.array_equal(db, db_ref)}, vs golden O1 {H.rel_rms(db, outs['dataBf']):.3e}")
+    assert err <= REF_TOL
+    assert np.allclose(mk, mk_ref, rtol=1e-6, atol=1e-6)
+    assert _errcount() == 0
+
+
+@pytest.mark.skipif(not H.have_ref_gpu("strict"), reason="oracle/_ref GPU build missing")
+def test_ref_compat_per_transmit_output(bf):
+    data, G, T, P, O, _ = load("ref6_rx_x")
+    r = H.prepare(data, G, T, P, {**O, "flagCompounding": False})
+    o2, m2 = H.run_ref_gpu(r, "strict")
+    db_ref, mk_ref = H.matlab_shape(r, o2, m2)
+    db, mk = run(bf, data, G, T, P, O, tableMode="ref_compat", flagCompounding=False)
+    assert db.shape == db_ref.shape
+    assert H.rel_rms(db, db_ref) <= REF_TOL
+    assert np.allclose(mk, mk_ref, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.skipif(not H.have_ref_gpu("fast"), reason="oracle/_ref GPU build missing")
+def test_report_reference_fast_math_build(bf):
+    """The reference as its wrapper compiles it (-use_fast_math): reported,
+    bounded loosely (fast-math trig on ~1e3 rad arguments)."""
+    data, G, T, P, O, _ = load("ref6_rx_x")
+    r = H.prepare(data, G, T, P, O)
+    o_fast, m_fast = H.run_ref_gpu(r, "fast")
+    o_str, _ = H.run_ref_gpu(r, "strict")
+    db, _ = run(bf, data, G, T, P, O, tableMode="ref_compat", flagCompounding=False)
+    db_fast, _ = H.matlab_shape(r, o_fast, m_fast)
+    e = H.rel_rms(db, db_fast)
+    print(f"REF_COMPAT vs reference -use_fast_math build: {e:.3e}; "
+          f"reference fast vs strict: {H.rel_rms(o_fast, o_str):.3e}")
+    assert e < 0.2
+
+
+# --------------------------------------------------------------------------
+# EXACT tables vs the FP64 oracle (physical synthetic data)
+# --------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def c0_small(cuda):
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c0", grid_scale=0.25, n_frame=3)
+    data = W.channel_data(w, seed=3, device="cuda").cpu().numpy()
+    g = w.groups[0]
+    return w, W.as_matlab(W.group_data(w, data, 0)), g.Geometry, g.Transmit, w.Param, w.Options
+
+
+INTERPS = [("quadratic", 0, H.INTERP_QUAD3), ("ref6", 0, H.INTERP_REF6), ("lanczos", 2, H.INTERP_LANCZOS),
+           ("lanczos", 3, H.INTERP_LANCZOS), ("lanczos", 4, H.INTERP_LANCZOS)]
+
+
+@pytest.mark.parametrize("interp,a,code", INTERPS)
+@pytest.mark.parametrize("storage,tol", [("float32", DB_FP32), ("float16", DB_FP16), ("bfloat16", DB_BF16)])
+def test_exact_vs_fp64_oracle(bf, c0_small, interp, a, code, storage, tol):
+    w, data, G, T, P, O = c0_small
+    r = H.prepare(data, G, T, P, O)
+    f64, m64 = H.run_fp64(r, code, a, data=np.asarray(data).transpose(3, 2, 1, 0).reshape(
+        r.n_frame, r.n_tx, r.n_ch, r.n_sample))
+    c64, cm64 = H.compound(f64, m64, True)
+    ref, mref = H.matlab_shape(r, c64, cm64)
+    db, mk = run(bf, data, G, T, P, O, interpolation=interp, lanczosOrder=max(a, 2), storage=storage)
+    rms, peak = H.error_db(db, ref)
+    print(f"EXACT {interp}{a or ''} {storage}: {rms:.1f} dB RMS, {peak:.1f} dB peak vs FP64")
+    assert rms <= tol
+    assert np.allclose(mk, mref, rtol=1e-5, atol=1e-4)
+
+
+def test_exact_receive_y_points_and_mask(bf):
+    for kw in (dict(receive_x=False, mask_tx=False), dict(receive_x=True, mask_tx=False, points=True),
+               dict(receive_x=False, mask_tx=True)):
+        data, G, T, P, O = case(7, lanczos=False, ns=128, **kw)
+        r = H.prepare(data, G, T, P, O)
+        f64, m64 = H.run_fp64(r, H.INTERP_QUAD3)
+        c, cm = H.compound(f64, m64, True)
+        ref, mref = H.matlab_shape(r, c, cm)
+        db, mk = run(bf, data, G, T, P, O)
+        rms, _ = H.error_db(db, ref)
+        print(kw, f"{rms:.1f} dB")
+        assert rms <= DB_FP32
+        # the cone test compares angles computed in FP64 on both sides
+        assert np.allclose(mk, mref, rtol=1e-5, atol=1e-4)
+
+
+def test_fused_equals_plain_and_frame_blocks(bf, c0_small):
+    w, data, G, T, P, O = c0_small
+    outs = {}
+    for kern, fb in (("plain", 0), ("fused", 1), ("fused", 2), ("fused", 4), ("fused", 8), ("fused", 16)):
+        outs[(kern, fb)], _ = run(bf, data, G, T, P, O, kernel=kern, framesPerBlock=fb)
+    base = outs[("plain", 0)]
+    for k, v in outs.items():
+        assert H.rel_rms(v, base) < 2e-6, (k, H.rel_rms(v, base))
+    assert _errcount() == 0
+
+
+def test_real_rf_input_and_torch_io(bf):
+    import torch
+    data, G, T, P, O, outs = load("ref6_real_rf")
+    db_np, _ = run(bf, data, G, T, P, O, tableMode="ref_compat")
+    db_t, mk_t = run(bf, torch.from_numpy(data).cuda(), G, T, P, O, tableMode="ref_compat")
+    assert isinstance(db_t, torch.Tensor) and db_t.is_cuda
+    assert np.array_equal(db_t.cpu().numpy(), db_np)
+    assert H.rel_rms(db_np, outs["dataBf"]) < 0.1
+
+
+def test_complex32_input_matches_fp16_storage(bf, c0_small):
+    import torch
+    w, data, G, T, P, O = c0_small
+    a, _ = run(bf, data, G, T, P, O, storage="float16")
+    t = torch.from_numpy(np.ascontiguousarray(data)).cuda().to(torch.complex32)
+    b, _ = run(bf, t, G, T, P, O)
+    assert H.rel_rms(b.cpu().numpy(), a) < 1e-6
+
+
+def test_batch_launch_equals_single_launches(bf, c0_small):
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200.params import normalize
+    w, data, G, T, P, O = c0_small
+    eng = bf.default_engine()
+    acqs = [normalize(data, G, T, P, {**O, "lanczosOrder": a}) for a in (4, 4)]
+    acqs[1].fnumber = 2.0
+    geoms = [eng.geometry(a) for a in acqs]
+    iq = torch.from_numpy(np.ascontiguousarray(np.asarray(data).transpose(3, 2, 1, 0))).cuda()
+    singles = [eng.beamform(g, iq, frames_per_block=4)[0].clone() for g in geoms]
+    outs, args, wss = [], [], []
+    for g in geoms:
+        o = torch.empty_like(singles[0])
+        a = eng.make_args(g, iq, iq_dtype=L.IQ_C64, n_sample=iq.shape[-1], n_frame=iq.shape[0], out=o,
+                          mask=None, compound=True, frames_per_block=4)
+        wss.append(torch.empty(eng.workspace_bytes(g, a), dtype=torch.uint8, device="cuda"))
+        outs.append(o)
+        args.append(a)
+    eng.run_batch(geoms, args, wss)
+    torch.cuda.synchronize()
+    for s, o in zip(singles, outs):
+        assert torch.equal(s, o)
+
+
+def test_bf_iq_rca_pmig_style(bf):
+    import torch
+    rng = np.random.default_rng(5)
+    raw = (rng.normal(size=(128, 32, 6)) + 1j * rng.normal(size=(128, 32, 6))).astype(np.complex64)
+    pmig = {"c": 1540, "fc": 7.8e6, "fsIQ": 15.6e6, "pitch": 0.3e-3, "theta": np.deg2rad([-3, 0, 3]),
+            "t0": -2e-6, "dx": 0.3e-3, "dz": 0.1e-3, "Nx": 16, "Nz": 24, "Zmin": 3e-3, "fnum": 1.0, "order": 8}
+    iq = bf.BfIQRCA(raw, pmig)
+    assert iq.shape == (24, 16, 2)
+    assert np.isfinite(iq).all() and np.abs(iq).max() > 0
