@@ -110,7 +110,9 @@ def _geom_key(acq: Acquisition, device: int) -> str:
     return h.hexdigest()
 
 
-_TORCH_IQ = {}
+# rcabf_iq_dtype -> (torch dtype of the buffer, buffer elements per I/Q sample)
+_IQ_TORCH = {L.IQ_C64: (torch.complex64, 1), L.IQ_C32: (torch.complex32, 1),
+             L.IQ_BF16X2: (torch.bfloat16, 2), L.IQ_RF_F32: (torch.float32, 2)}
 
 
 def _iq_dtype_of(t: "torch.Tensor", layout: str) -> int:
@@ -175,6 +177,23 @@ class Engine:
                   n_frame: int, out: "torch.Tensor", mask: "torch.Tensor | None", compound: bool,
                   storage: int = L.STORE_F32, kernel: int = L.KERNEL_AUTO, accumulate: bool = False,
                   frames_per_block: int = 0) -> L.BeamformArgs:
+        # The C ABI takes raw pointers: check every buffer holds what the
+        # sizes claim before handing it over.
+        T = 1 if compound else geom.n_tx
+        dt, per_sample = _IQ_TORCH[iq_dtype]
+        if iq.dtype != dt:
+            raise ValueError(f"channel data dtype {iq.dtype} does not match iq_dtype {iq_dtype} ({dt})")
+        need_in = n_frame * geom.n_tx * geom.n_ele * n_sample * per_sample
+        if n_frame < 1 or n_sample < 1 or iq.numel() < need_in or not iq.is_contiguous():
+            raise ValueError(f"channel data holds {iq.numel()} elements, {need_in} needed "
+                             f"({n_frame} frames x {geom.n_tx} tx x {geom.n_ele} elements x {n_sample} samples)")
+        if out.dtype != torch.complex64 or out.numel() < n_frame * T * geom.n_pix or not out.is_contiguous():
+            raise ValueError("out must be a contiguous complex64 tensor of frames x (1 or tx) x pixels")
+        if mask is not None and (mask.dtype != torch.float32 or mask.numel() < T * geom.n_pix):
+            raise ValueError("mask must be a float32 tensor of (1 or tx) x pixels")
+        for t in (iq, out) + ((mask,) if mask is not None else ()):
+            if t.device != self.device:
+                raise ValueError(f"tensor on {t.device}, engine on {self.device}")
         a = L.BeamformArgs()
         a.struct_size = C.sizeof(L.BeamformArgs)
         a.iq_dtype = iq_dtype

@@ -163,8 +163,9 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
 {
     DeviceState *ds = device_state(g0->device);
     prm.err_count = ds->err;
-    const std::array<int64_t, 5> key{g0->mode, g0->kind, p.fb, p.store, (int64_t)prm.wmax * prm.row_words * 4};
-    const size_t smem = (size_t)key[4];
+    // every stage buffer holds wmax rows of row_words words
+    const size_t smem = (size_t)FUSED_STAGES * prm.wmax * prm.row_words * 4;
+    const std::array<int64_t, 5> key{g0->mode, g0->kind, p.fb, p.store, (int64_t)smem};
     int occ;
     {
         std::lock_guard<std::mutex> lk(ds->mu);

@@ -337,6 +337,16 @@ fused_das_kernel(const __grid_constant__ FusedParams prm)
     const int tid = threadIdx.x;
     const int stage_bytes = prm.wmax * prm.row_words * 4;
     const int stride_s = prm.row_words * 4;
+    {
+        // The launch must provide FUSED_STAGES window buffers; if it did not,
+        // record the error and touch nothing (uniform across the block).
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (dyn < (unsigned)(FUSED_STAGES * stage_bytes) || stride_s < ROWB) {
+            if (tid == 0) atomicAdd(prm.err_count, 1ull);
+            return;
+        }
+    }
 
     for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x) {
         int ji = 0;

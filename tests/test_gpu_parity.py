@@ -184,11 +184,12 @@ def test_batch_launch_equals_single_launches(bf, c0_small):
     acqs[1].fnumber = 2.0
     geoms = [eng.geometry(a) for a in acqs]
     iq = torch.from_numpy(np.ascontiguousarray(np.asarray(data).transpose(3, 2, 1, 0))).cuda()
+    iq = iq.reshape(w.n_frame, w.n_tx, w.n_ele, w.n_sample)          # [frame][tx][element][sample]
     singles = [eng.beamform(g, iq, frames_per_block=4)[0].clone() for g in geoms]
     outs, args, wss = [], [], []
     for g in geoms:
         o = torch.empty_like(singles[0])
-        a = eng.make_args(g, iq, iq_dtype=L.IQ_C64, n_sample=iq.shape[-1], n_frame=iq.shape[0], out=o,
+        a = eng.make_args(g, iq, iq_dtype=L.IQ_C64, n_sample=w.n_sample, n_frame=w.n_frame, out=o,
                           mask=None, compound=True, frames_per_block=4)
         wss.append(torch.empty(eng.workspace_bytes(g, a), dtype=torch.uint8, device="cuda"))
         outs.append(o)
