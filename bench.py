@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2")
+    ap.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling cases)")
     ap.add_argument("--storage", default=None, help="float32 | float16 | bfloat16 (default: workload's)")
     ap.add_argument("--kernel", default="fused", choices=["fused", "plain"])
     ap.add_argument("--frames-per-block", type=int, default=0)
@@ -207,7 +208,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
-    w = W.get(a.workload)
+    w = W.get(a.workload, n_frame=a.frames)
     storage = a.storage or w.storage
     st_code = {"float32": L.STORE_F32, "float16": L.STORE_F16, "bfloat16": L.STORE_BF16}[storage]
     kern = L.KERNEL_PLAIN if a.kernel == "plain" else L.KERNEL_FUSED

@@ -63,11 +63,43 @@ TileShape default_tile(const rcabf_geometry *g)
     return TileShape{tu, tv, tz};
 }
 
-int choose_fb(int64_t n_frame, int requested)
+bool fb_supported(int mode, int fb)
 {
-    if (requested > 0) return requested;
-    if (n_frame >= 8) return 8;
-    return pow2_ceil(n_frame);
+    switch (fb) {
+    case 1: case 2: case 4: case 8: case 16: return true;
+    case 24: case 32: case 40: return mode == MODE_EXACT;
+    default: return false;
+    }
+}
+
+// Rows one staging buffer can hold at frame block fb.
+static int stage_capacity_rows(const rcabf_geometry *g, int store, int fb)
+{
+    const size_t tbl = fused_table_bytes(g->mode, g->kind);
+    const int cap = (int)((SMEM_BUDGET - tbl) / ((size_t)fused_stages(store) * fused_row_words(fb) * 4));
+    return std::min(cap, fused_stage_rows_cap(store, fb));
+}
+
+// Frame block: each block repeats the per-(voxel, rx, tx) setup, worth about
+// SETUP_FRAMES frames of work, and pads the last block; pick the block that
+// minimises blocks x (FB + SETUP_FRAMES) among the compiled sizes whose
+// staging buffers hold the largest window (`need` rows).  0 = none fits.
+int choose_fb(const rcabf_geometry *g, int store, int64_t n_frame, int requested, int need)
+{
+    const int cands[] = {1, 2, 4, 8, 16, 24, 32, 40};
+    const double SETUP_FRAMES = 4.0;
+    int best = 0;
+    double best_cost = 1e300;
+    for (int fb : cands) {
+        if (!fb_supported(g->mode, fb)) continue;
+        if (requested > 0 && fb > requested) continue;
+        if (requested <= 0 && fb > 2 * n_frame && fb > 1) continue;
+        if (stage_capacity_rows(g, store, fb) < need) continue;
+        const double blocks = (double)((n_frame + fb - 1) / fb);
+        const double cost = requested > 0 ? -fb : blocks * (fb + SETUP_FRAMES);
+        if (cost < best_cost - 1e-9) { best_cost = cost; best = fb; }
+    }
+    return best;
 }
 
 int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
@@ -81,8 +113,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
     if (a->storage < RCABF_STORE_F32 || a->storage > RCABF_STORE_BF16) return RCABF_ERR_INVALID_ARGUMENT;
     if (g->mode == MODE_REF && a->storage != RCABF_STORE_F32) return RCABF_ERR_UNSUPPORTED;
     const int fb_req = a->frames_per_block;
-    if (fb_req != 0 && fb_req != 1 && fb_req != 2 && fb_req != 4 && fb_req != 8 && fb_req != 16)
-        return RCABF_ERR_INVALID_ARGUMENT;
+    if (fb_req != 0 && !fb_supported(g->mode, fb_req)) return RCABF_ERR_INVALID_ARGUMENT;
     p = Plan{};
     p.kernel = (a->kernel == RCABF_KERNEL_PLAIN) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
     if (p.kernel == RCABF_KERNEL_PLAIN) {
@@ -90,19 +121,25 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
         return RCABF_OK;
     }
     p.store = a->storage;
-    p.fb = choose_fb(a->n_frame, fb_req);
-    p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
     p.ts = default_tile(g);
+    // the largest window of any (tile, tx, rx) step, rounded up: the staging
+    // buffers hold it, so the kernel never needs a fallback path
+    const int need = std::min<int64_t>(g->window_rows(p.ts), a->n_sample);
+    p.fb = choose_fb(g, p.store, a->n_frame, fb_req, need);
+    if (p.fb == 0) {  // no staging buffer holds the window: one-frame kernel
+        p.kernel = RCABF_KERNEL_PLAIN;
+        p.total = 0;
+        return RCABF_OK;
+    }
+    p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
     p.tiles_z = (int)((g->n_z + p.ts.tz - 1) / p.ts.tz);
     p.tiles_u = (int)((g->n_u + p.ts.tu - 1) / p.ts.tu);
     p.tiles_v = (int)((g->n_v + p.ts.tv - 1) / p.ts.tv);
     const int es = store_bytes(p.store);
     const int rowb = p.fb * es;
-    p.row_words = rowb >= 16 ? (rowb + 16) / 4 : rowb / 4;
-    const int want = g->window_rows(p.ts);
-    const int cap = (int)(SMEM_BUDGET / (FUSED_STAGES * p.row_words * 4));
-    p.wmax = std::max(kind_taps(g->kind), std::min(want, cap));
-    p.smem = (size_t)FUSED_STAGES * p.wmax * p.row_words * 4;
+    p.row_words = fused_row_words(p.fb);
+    p.wmax = std::max(kind_taps(g->kind), need);
+    p.smem = fused_smem_bytes(g->mode, g->kind, p.store, p.wmax, p.row_words);
     p.slab_bytes = ((int64_t)a->n_sample * rowb + 15) / 16 * 16;
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     size_t off = 0;
@@ -163,8 +200,7 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
 {
     DeviceState *ds = device_state(g0->device);
     prm.err_count = ds->err;
-    // every stage buffer holds wmax rows of row_words words
-    const size_t smem = (size_t)FUSED_STAGES * prm.wmax * prm.row_words * 4;
+    const size_t smem = fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
     const std::array<int64_t, 5> key{g0->mode, g0->kind, p.fb, p.store, (int64_t)smem};
     int occ;
     {
@@ -365,6 +401,8 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_bea
         if (s != RCABF_OK) return s;
         if ((s = check_ptrs(&as[i], p)) != RCABF_OK) return s;
         if (i == 0) p0 = p;
+        // one launch = one kernel variant: every job fused, same frame block
+        if (p.kernel != RCABF_KERNEL_FUSED || p.fb != p0.fb) return RCABF_ERR_UNSUPPORTED;
         wmax = std::max(wmax, p.wmax);
         if ((s = stage_job(g, &as[i], p, prm.jobs[i], st)) != RCABF_OK) return s;
         prm.jobs[i].item_begin = items;

@@ -29,8 +29,17 @@ static cudaError_t fused_fb(int fb, const FusedParams *p, int grid, size_t smem,
     case 4: return fused_do<MODE, KIND, 4, STORE>(p, grid, smem, st, what, occ);
     case 8: return fused_do<MODE, KIND, 8, STORE>(p, grid, smem, st, what, occ);
     case 16: return fused_do<MODE, KIND, 16, STORE>(p, grid, smem, st, what, occ);
-    default: return cudaErrorInvalidValue;
+    default: break;
     }
+    if constexpr (MODE == MODE_EXACT) {   // wider frame blocks: exact tables only
+        switch (fb) {
+        case 24: return fused_do<MODE, KIND, 24, STORE>(p, grid, smem, st, what, occ);
+        case 32: return fused_do<MODE, KIND, 32, STORE>(p, grid, smem, st, what, occ);
+        case 40: return fused_do<MODE, KIND, 40, STORE>(p, grid, smem, st, what, occ);
+        default: break;
+        }
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <int MODE, int KIND, int IQ>

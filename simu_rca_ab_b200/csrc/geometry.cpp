@@ -54,6 +54,32 @@ static inline void unit_phasor(double cycles, float &c, float &s)
     s = (float)std::sin(2.0 * M_PI * r);
 }
 
+// Polyphase weight table of a windowed-sinc kernel, sinc(x) sinc(x / W) at
+// x_j = d + LO - j (RCA.cu:331-336 for W = 2, 6 taps; Lanczos-a for W = a,
+// zero for |x| >= a): WT_Q rows of 16 floats, the weights at d = q / WT_Q
+// then their increments to d = (q + 1) / WT_Q, evaluated in FP64.
+static std::vector<float> weight_table(int kind)
+{
+    const int Q = 256, ROW = 16;
+    const int taps = kind_taps(kind), lo = kind_lo(kind);
+    const double W = kind == K_REF6 ? 2.0 : kind == K_LANCZOS2 ? 2.0 : kind == K_LANCZOS3 ? 3.0 : 4.0;
+    const bool lanczos = kind != K_REF6;
+    auto sinc = [](double x) { return x == 0.0 ? 1.0 : std::sin(M_PI * x) / (M_PI * x); };
+    auto w = [&](double d, int j) {
+        const double x = d + lo - j;
+        if (lanczos && std::fabs(x) >= W) return 0.0;
+        return sinc(x) * sinc(x / W);
+    };
+    std::vector<float> t((size_t)Q * ROW, 0.f);
+    for (int q = 0; q < Q; ++q)
+        for (int j = 0; j < taps; ++j) {
+            const double a = w((double)q / Q, j), b = w((double)(q + 1) / Q, j);
+            t[(size_t)q * ROW + j] = (float)a;
+            t[(size_t)q * ROW + 8 + j] = (float)(b - a);
+        }
+    return t;
+}
+
 template <typename T>
 static cudaError_t upload(T **dst, const std::vector<T> &src, cudaStream_t st)
 {
@@ -75,6 +101,7 @@ void free_geometry(rcabf_geometry *g)
     cudaFree(g->apod_sum);
     cudaFree(g->ab);
     cudaFree(g->ab_ph);
+    cudaFree(g->wtab);
     cudaSetDevice(prev);
     delete g;
 }
@@ -395,6 +422,11 @@ int build_geometry(const rcabf_geometry_desc *d, cudaStream_t st, rcabf_geometry
             if ((ce = cudaStreamSynchronize(st)) != cudaSuccess) goto cuda_fail;
         }
     }
+    if (mode == MODE_EXACT && kind != K_QUAD3) {
+        std::vector<float> wt = weight_table(kind);
+        if ((ce = upload(&g->wtab, wt, st)) != cudaSuccess) goto cuda_fail;
+        if ((ce = cudaStreamSynchronize(st)) != cudaSuccess) goto cuda_fail;
+    }
     g->has_ab = d->ab_law ? 1 : 0;
     g->ab_per_tx = d->ab_per_tx ? 1 : 0;
     *out = g.release();
@@ -413,6 +445,7 @@ rcabf::DevGeom rcabf_geometry::dev() const
     rcabf::DevGeom d{};
     d.rx_tab = rx_tab; d.tx_tab = tx_tab; d.cone_u = cone_u; d.apod_sum = apod_sum;
     d.ab = ab; d.ab_ph = ab_ph; d.ab_per_tx = ab_per_tx; d.mode = mode;
+    d.wtab = wtab;
     d.n_ele = n_ele; d.n_tx = n_tx;
     d.n_z = n_z; d.n_u = n_u; d.n_v = n_v; d.s_z = s_z; d.s_u = s_u; d.s_v = s_v; d.n_pix = n_pix;
     d.ref = ref;

@@ -58,6 +58,7 @@ struct rcabf_geometry {
     float *apod_sum = nullptr;
     float *ab = nullptr;
     float2 *ab_ph = nullptr;
+    float *wtab = nullptr;
     rcabf::RefScalars ref{};
 
     std::mutex mu;

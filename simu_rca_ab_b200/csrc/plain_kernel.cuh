@@ -1,0 +1,99 @@
+// Plain delay-and-sum kernel: one launch per frame, one thread per voxel,
+// tables and channel data read straight from global memory (the comparator
+// for the fused kernel, and the one-frame path).
+#pragma once
+
+#include "das_common.cuh"
+
+namespace rcabf {
+
+// ------------------------------------------------------------------------
+// Plain kernel: one launch per frame, one thread per voxel
+// ------------------------------------------------------------------------
+template <int IQ>
+__device__ __forceinline__ float2 load_iq(const void *base, int64_t i)
+{
+    if constexpr (IQ == 0) return __ldg(reinterpret_cast<const float2 *>(base) + i);
+    else if constexpr (IQ == 1) return __half22float2(reinterpret_cast<const __half2 *>(base)[i]);
+    else if constexpr (IQ == 2) return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162 *>(base)[i]);
+    else {  // real RF, Q negated (RCA.m:476)
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(base) + i);
+        return make_float2(v.x, -v.y);
+    }
+}
+
+template <int MODE, int KIND, int IQ>
+__global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ PlainParams prm)
+{
+    using KT = KindTraits<KIND>;
+    const DevGeom &g = prm.g;
+    const int64_t n_vox = g.n_z * g.n_u * g.n_v;
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_vox) return;
+    const int64_t iz = v % g.n_z;
+    const int64_t iu = (v / g.n_z) % g.n_u;
+    const int64_t iv = v / (g.n_z * g.n_u);
+    const int64_t rxkey = iu * g.n_z + iz, txkey = iv * g.n_z + iz;
+    const int64_t n_rxkey = g.n_u * g.n_z, n_txkey = g.n_v * g.n_z;
+    const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
+    float2 acc[1] = {make_float2(0.f, 0.f)};
+    float2 acc_tx[1] = {make_float2(0.f, 0.f)};
+    for (int tx = 0; tx < g.n_tx; ++tx) {
+        const float4 t = __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey]);
+        bool cone_ok = ((MODE == MODE_EXACT) ? t.w : t.y) != 0.0f;
+        if (g.cone_u != nullptr) cone_ok = cone_ok && g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
+        if (cone_ok) {
+            const int64_t chan0 = (prm.frame * g.n_tx + tx) * (int64_t)g.n_ele;
+            for (int rx = 0; rx < g.n_ele; ++rx) {
+                const float4 e = __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]);
+                const float ab = ab_value(g, tx, rx);
+                Setup<KIND> st;
+                if constexpr (MODE == MODE_EXACT)
+                    setup_exact<KIND>(t, e, ab, ab_phasor(g, tx, rx), prm.n_sample, st);
+                else
+                    setup_ref<KIND>(t, e, ab, g.ref, prm.n_sample, st);
+                if (!st.ok) continue;
+                const int64_t base = (chan0 + rx) * prm.n_sample + st.n0 - KT::LO;
+                float2 tsum = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < KT::TAPS; ++j) {
+                    const float2 x = load_iq<IQ>(prm.iq, base + j);
+                    if constexpr (MODE == MODE_EXACT) {
+                        tsum.x = fmaf(st.w[j], x.x, tsum.x);
+                        tsum.y = fmaf(st.w[j], x.y, tsum.y);
+                    } else if (j == 0) {
+                        tsum = make_float2(__fmul_rn(st.w[0], x.x), __fmul_rn(st.w[0], x.y));
+                    } else {
+                        tsum.x = __fadd_rn(tsum.x, __fmul_rn(st.w[j], x.x));
+                        tsum.y = __fadd_rn(tsum.y, __fmul_rn(st.w[j], x.y));
+                    }
+                }
+                float2 &a = acc_tx[0];
+                if constexpr (MODE == MODE_EXACT) {
+                    a.x = fmaf(st.P.x, tsum.x, fmaf(-st.P.y, tsum.y, a.x));
+                    a.y = fmaf(st.P.x, tsum.y, fmaf(st.P.y, tsum.x, a.y));
+                } else {
+                    const float cs = st.P.x, sn = st.P.y;
+                    a.x = __fadd_rn(a.x, __fmul_rn(st.apod, __fadd_rn(__fmul_rn(tsum.x, cs), __fmul_rn(tsum.y, sn))));
+                    a.y = __fadd_rn(a.y, __fmul_rn(st.apod, __fadd_rn(__fmul_rn(-tsum.x, sn), __fmul_rn(tsum.y, cs))));
+                }
+            }
+        }
+        if (!prm.compound) {
+            float2 *o = prm.out + (prm.frame * g.n_tx + tx) * g.n_pix + pix;
+            if (prm.accumulate) { float2 q = *o; q.x += acc_tx[0].x; q.y += acc_tx[0].y; *o = q; }
+            else *o = acc_tx[0];
+        } else {
+            acc[0].x = __fadd_rn(acc[0].x, acc_tx[0].x);
+            acc[0].y = __fadd_rn(acc[0].y, acc_tx[0].y);
+        }
+        acc_tx[0] = make_float2(0.f, 0.f);
+    }
+    if (prm.compound) {
+        float2 *o = prm.out + prm.frame * g.n_pix + pix;
+        if (prm.accumulate) { float2 q = *o; q.x += acc[0].x; q.y += acc[0].y; *o = q; }
+        else *o = acc[0];
+    }
+}
+
+}  // namespace rcabf

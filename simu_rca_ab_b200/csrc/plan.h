@@ -9,8 +9,8 @@
 
 namespace rcabf {
 
-// Shared memory the fused kernel's window buffers may take per CTA.
-constexpr size_t SMEM_BUDGET = 96 * 1024;
+// Shared memory the fused kernel may take per CTA (two CTAs fit an SM).
+constexpr size_t SMEM_BUDGET = 110 * 1024;
 
 struct Plan {
     int kernel = 0;       // rcabf_kernel
@@ -26,5 +26,28 @@ struct Plan {
 };
 
 int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p);
+
+// Frame-block sizes with a compiled fused-kernel variant.
+bool fb_supported(int mode, int fb);
+
+// Shared-memory layout of the fused kernel (fused_kernel.cuh): the polyphase
+// weight table (EXACT windowed-sinc kinds) followed by the window buffers --
+// three for complex64 slabs (cp.async pipeline), two for FP16/BF16 slabs
+// (register staging) -- each wmax rows of row_words 4-byte words.
+inline int fused_stages(int store) { return store == ST_F32 ? 3 : 2; }
+inline size_t fused_table_bytes(int mode, int kind) { return (mode == MODE_EXACT && kind != K_QUAD3) ? 16384 : 0; }
+inline size_t fused_smem_bytes(int mode, int kind, int store, int wmax, int row_words)
+{
+    return fused_table_bytes(mode, kind) + (size_t)fused_stages(store) * wmax * row_words * 4;
+}
+// Staged rows are FP32 (8 bytes per frame), padded by 16 bytes when >= 16.
+inline int fused_row_words(int fb) { return fb * 8 >= 16 ? (fb * 8 + 16) / 4 : (fb * 8) / 4; }
+// Register staging holds at most 4 x 16-byte chunks per thread (256 threads).
+inline int fused_stage_rows_cap(int store, int fb)
+{
+    if (store == ST_F32) return 1 << 30;
+    const int rawb = fb * 4, cs = rawb < 16 ? rawb : 16;
+    return 4 * 256 / (rawb / cs);
+}
 
 }  // namespace rcabf

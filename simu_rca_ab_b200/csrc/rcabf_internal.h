@@ -63,6 +63,7 @@ struct DevGeom {
     const float *apod_sum;
     const float *ab;           // NULL when no aberration law
     const float2 *ab_ph;       // EXACT only
+    const float *wtab;         // EXACT windowed-sinc kinds: polyphase weight table (WT_Q x 16 floats)
     int32_t ab_per_tx;
     int32_t mode;
     int32_t n_ele, n_tx;

@@ -144,14 +144,20 @@ def test_exact_receive_y_points_and_mask(bf):
         assert np.allclose(mk, mref, rtol=1e-5, atol=1e-4)
 
 
-def test_fused_equals_plain_and_frame_blocks(bf, c0_small):
+@pytest.mark.parametrize("storage", ["float32", "float16", "bfloat16"])
+def test_fused_equals_plain_and_frame_blocks(bf, c0_small, storage):
+    """Frame blocking does not change any frame's arithmetic: every fused
+    variant gives identical bits.  The plain kernel evaluates the window
+    directly instead of through the polyphase table: within 1e-4 (-80 dB)."""
     w, data, G, T, P, O = c0_small
     outs = {}
-    for kern, fb in (("plain", 0), ("fused", 1), ("fused", 2), ("fused", 4), ("fused", 8), ("fused", 16)):
-        outs[(kern, fb)], _ = run(bf, data, G, T, P, O, kernel=kern, framesPerBlock=fb)
-    base = outs[("plain", 0)]
-    for k, v in outs.items():
-        assert H.rel_rms(v, base) < 2e-6, (k, H.rel_rms(v, base))
+    for fb in (1, 2, 4, 8, 16, 24, 32, 40):
+        outs[fb], _ = run(bf, data, G, T, P, O, kernel="fused", framesPerBlock=fb, storage=storage)
+    plain, _ = run(bf, data, G, T, P, O, kernel="plain", storage=storage)
+    for fb, v in outs.items():
+        assert np.array_equal(v, outs[1]), fb
+    if storage == "float32":
+        assert H.rel_rms(outs[8], plain) < 1e-4, H.rel_rms(outs[8], plain)
     assert _errcount() == 0
 
 
