@@ -75,6 +75,9 @@ typedef enum rcabf_status {
 
 const char *rcabf_status_string(int status);
 int rcabf_abi_version(void);
+/* Detail of the calling thread's last RCABF_ERR_CUDA: the failing step and
+ * CUDA's error string ("" if none).  No reference counterpart. */
+const char *rcabf_last_error(void);
 
 /* ------------------------------------------------------------------------ */
 /* Enumerations                                                              */

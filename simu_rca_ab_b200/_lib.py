@@ -68,6 +68,7 @@ class BeamformArgs(C.Structure):
 _SIGS = {
     "rcabf_status_string": (C.c_char_p, [C.c_int]),
     "rcabf_abi_version": (C.c_int, []),
+    "rcabf_last_error": (C.c_char_p, []),
     "rcabf_create_geometry": (C.c_int, [C.POINTER(GeometryDesc), C.c_void_p, C.POINTER(C.c_void_p)]),
     "rcabf_destroy_geometry": (C.c_int, [C.c_void_p]),
     "rcabf_geometry_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -110,7 +111,9 @@ class RcabfError(RuntimeError):
     def __init__(self, status: int, where: str = ""):
         self.status = int(status)
         self.identifier = lib().rcabf_status_string(int(status)).decode()
-        super().__init__(f"{self.identifier} (status {self.status}){': ' + where if where else ''}")
+        detail = lib().rcabf_last_error().decode() if self.status == 106 else ""
+        super().__init__(f"{self.identifier} (status {self.status}){': ' + where if where else ''}"
+                         f"{' -- ' + detail if detail else ''}")
 
 
 def check(status: int, where: str = "") -> None:

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -19,6 +20,15 @@ using namespace rcabf;
 namespace rcabf {
 
 std::atomic<int64_t> g_launches{0};
+
+// Detail of the last RCABF_ERR_CUDA of this thread (rcabf_last_error()).
+static thread_local char g_last_err[256] = "";
+
+static int cuda_fail(cudaError_t e, const char *where)
+{
+    snprintf(g_last_err, sizeof(g_last_err), "%s: %s (cudaError %d)", where, cudaGetErrorString(e), (int)e);
+    return RCABF_ERR_CUDA;
+}
 
 struct DeviceState {
     unsigned long long *err = nullptr;
@@ -168,17 +178,18 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
     ip.iq = a->iq; ip.iq_dtype = a->iq_dtype; ip.n_sample = (int)a->n_sample; ip.n_ele = g->n_ele;
     ip.n_tx = g->n_tx; ip.n_frame = a->n_frame; ip.fb = p.fb; ip.n_fb = p.n_fb;
     ip.S = ws + p.off_S; ip.slab_bytes = p.slab_bytes;
-    if (launch_ingest(ip, p.store, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    cudaError_t ce = launch_ingest(ip, p.store, st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "ingest launch");
     if (marks) mark(marks, 1, st);
     RangeParams rr{};
     rr.tab = g->rx_tab; rr.out = reinterpret_cast<float2 *>(ws + p.off_rxr); rr.rows = g->n_ele;
     rr.n_a = g->n_u; rr.n_z = g->n_z; rr.ta = p.ts.tu; rr.tz = p.ts.tz; rr.tiles_a = p.tiles_u;
     rr.tiles_z = p.tiles_z; rr.mode = g->mode; rr.is_rx = 1;
-    if (launch_range(rr, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    if ((ce = launch_range(rr, st)) != cudaSuccess) return cuda_fail(ce, "rx range launch");
     RangeParams tr = rr;
     tr.tab = g->tx_tab; tr.out = reinterpret_cast<float2 *>(ws + p.off_txr); tr.rows = g->n_tx;
     tr.n_a = g->n_v; tr.ta = p.ts.tv; tr.tiles_a = p.tiles_v; tr.is_rx = 0;
-    if (launch_range(tr, st) != cudaSuccess) return RCABF_ERR_CUDA;
+    if ((ce = launch_range(tr, st)) != cudaSuccess) return cuda_fail(ce, "tx range launch");
     g_launches += 3;
     if (marks) mark(marks, 2, st);
 
@@ -206,7 +217,8 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     {
         std::lock_guard<std::mutex> lk(ds->mu);
         if (!ds->prepared[key]) {
-            if (prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem) != cudaSuccess) return RCABF_ERR_CUDA;
+            const cudaError_t pe = prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
+            if (pe != cudaSuccess) return cuda_fail(pe, "fused kernel shared-memory attribute");
             ds->prepared[key] = true;
             ds->occ[key] = fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
         }
@@ -214,8 +226,8 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     }
     const int64_t grid = std::min<int64_t>(prm.n_items, (int64_t)ds->n_sm * occ);
     if (grid <= 0) return RCABF_OK;
-    if (launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st) != cudaSuccess)
-        return RCABF_ERR_CUDA;
+    const cudaError_t le = launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st);
+    if (le != cudaSuccess) return cuda_fail(le, "fused kernel launch");
     g_launches += 1;
     return RCABF_OK;
 }
@@ -249,7 +261,8 @@ int beamform_one(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t s
         pp.err_count = device_state(g->device)->err;
         for (int64_t f = 0; f < a->n_frame; ++f) {
             pp.frame = f;
-            if (launch_plain(g->mode, g->kind, pp, st) != cudaSuccess) return RCABF_ERR_CUDA;
+            const cudaError_t le = launch_plain(g->mode, g->kind, pp, st);
+            if (le != cudaSuccess) return cuda_fail(le, "plain kernel launch");
             g_launches += 1;
         }
     } else {
@@ -264,8 +277,8 @@ int beamform_one(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t s
     }
     mark(a, 3, st);
     if (a->mask) {
-        if (launch_mask(g->dev(), a->mask, a->compound ? 1 : 0, a->accumulate ? 1 : 0, st) != cudaSuccess)
-            return RCABF_ERR_CUDA;
+        const cudaError_t me = launch_mask(g->dev(), a->mask, a->compound ? 1 : 0, a->accumulate ? 1 : 0, st);
+        if (me != cudaSuccess) return cuda_fail(me, "mask kernel launch");
         g_launches += 1;
     }
     mark(a, 4, st);
@@ -326,6 +339,8 @@ const char *rcabf_status_string(int s)
 }
 
 int rcabf_abi_version(void) { return RCABF_ABI_VERSION; }
+
+const char *rcabf_last_error(void) { return g_last_err; }
 
 int rcabf_create_geometry(const rcabf_geometry_desc *desc, void *stream, rcabf_geometry **out)
 {
@@ -416,9 +431,8 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_bea
     if (s != RCABF_OK) return s;
     for (int i = 0; i < n; ++i) {
         if (!as[i].mask) continue;
-        if (launch_mask(gs[i]->dev(), as[i].mask, as[i].compound ? 1 : 0, as[i].accumulate ? 1 : 0, st) !=
-            cudaSuccess)
-            return RCABF_ERR_CUDA;
+        const cudaError_t me = launch_mask(gs[i]->dev(), as[i].mask, as[i].compound ? 1 : 0, as[i].accumulate ? 1 : 0, st);
+        if (me != cudaSuccess) return cuda_fail(me, "mask kernel launch");
         g_launches += 1;
     }
     return RCABF_OK;

@@ -22,7 +22,7 @@ template <> __device__ __forceinline__ __half2 from_f2<ST_F16>(float2 v) { retur
 template <> __device__ __forceinline__ __nv_bfloat162 from_f2<ST_BF16>(float2 v) { return __float22bfloat162_rn(v); }
 
 constexpr int INGEST_NS = 64;
-constexpr int INGEST_MAX_FB = 32;
+constexpr int INGEST_MAX_FB = 64;
 
 template <int STORE, int IQ>
 __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p)
