@@ -241,6 +241,7 @@ def main():
         args.append(ar)
     ws = [torch.empty(max(256, eng.workspace_bytes(g, ar)), dtype=torch.uint8, device=dev)
           for g, ar in zip(geoms, args)]
+    plan = eng.plan(geoms[0], args[0])
 
     def step():
         for g, ar, wsp in zip(geoms, args, ws):
@@ -373,7 +374,8 @@ def main():
                                    f"grid {w.grid_shape[1]}x{w.grid_shape[2]}x{w.grid_shape[0]}, Lanczos a={w.lanczos_a}, "
                                    f"f-number {w.Param['fnumber']}",
                        "storage": storage, "kernel": a.kernel, "l2": "inputs larger than L2 (no flush needed)",
-                       "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)"},
+                       "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)",
+                       "plan": plan},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,

@@ -116,8 +116,10 @@ typedef enum rcabf_storage {
 
 typedef enum rcabf_kernel {
     RCABF_KERNEL_AUTO = 0,  /* fused tiled kernel */
-    RCABF_KERNEL_FUSED = 1, /* persistent voxel-tiled shared-memory gather, all frames in one launch */
-    RCABF_KERNEL_PLAIN = 2  /* one launch per frame, one thread per voxel, global gathers */
+    RCABF_KERNEL_FUSED = 1, /* persistent voxel-tiled shared-memory gather, all frames in one launch;
+                               voxel-blocked along the steering axis when the geometry allows */
+    RCABF_KERNEL_PLAIN = 2, /* one launch per frame, one thread per voxel, global gathers */
+    RCABF_KERNEL_FUSED_NOBLOCK = 3 /* the fused kernel with one voxel per thread */
 } rcabf_kernel;
 
 /* ------------------------------------------------------------------------ */
@@ -213,6 +215,11 @@ typedef struct rcabf_beamform_args {
 
 /* Scratch bytes rcabf_beamform needs for these arguments. */
 int rcabf_beamform_workspace_size(const rcabf_geometry *g, const rcabf_beamform_args *a, size_t *bytes);
+
+/* The launch plan rcabf_beamform would use for these arguments, as a JSON
+ * object (kernel, frames per block, tile, window rows, shared memory,
+ * workspace) written into buf (NUL-terminated, truncated to len). */
+int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, char *buf, size_t len);
 
 /* Beamforms every frame and transmit of one acquisition.  Replaces the
  * chunked feval/gather loop of bfVirtualSourceGeneric_RCA.m:640-711 and the

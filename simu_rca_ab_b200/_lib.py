@@ -18,7 +18,7 @@ TABLES_EXACT, TABLES_REF_COMPAT = 0, 1
 GRID_RECTILINEAR, GRID_POINTS = 0, 1
 IQ_C64, IQ_C32, IQ_BF16X2, IQ_RF_F32 = 0, 1, 2, 3
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
-KERNEL_AUTO, KERNEL_FUSED, KERNEL_PLAIN = 0, 1, 2
+KERNEL_AUTO, KERNEL_FUSED, KERNEL_PLAIN, KERNEL_FUSED_NOBLOCK = 0, 1, 2, 3
 
 OK = 0
 ERR_OOM_ADMISSION = 104
@@ -76,6 +76,7 @@ _SIGS = {
     "rcabf_geometry_sources": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "rcabf_beamform_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.POINTER(C.c_size_t)]),
     "rcabf_beamform": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
+    "rcabf_describe_plan": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_char_p, C.c_size_t]),
     "rcabf_beamform_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),

@@ -208,6 +208,13 @@ class Engine:
         a.frames_per_block = frames_per_block
         return a
 
+    def plan(self, geom: GeometryHandle, a: L.BeamformArgs) -> dict:
+        """The launch plan librcabf picks for these arguments."""
+        import json
+        buf = C.create_string_buffer(1024)
+        L.check(L.lib().rcabf_describe_plan(C.c_void_p(geom.ptr), C.byref(a), buf, 1024), "rcabf_describe_plan")
+        return json.loads(buf.value.decode())
+
     def workspace_bytes(self, geom: GeometryHandle, a: L.BeamformArgs) -> int:
         n = C.c_size_t()
         L.check(L.lib().rcabf_beamform_workspace_size(C.c_void_p(geom.ptr), C.byref(a), C.byref(n)),

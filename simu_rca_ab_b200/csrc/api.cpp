@@ -131,6 +131,59 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
         return RCABF_OK;
     }
     p.store = a->storage;
+    const int es = store_bytes(p.store);
+    auto layout = [&](int tile_v_extent) {
+        p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
+        p.tiles_z = (int)((g->n_z + p.ts.tz - 1) / p.ts.tz);
+        p.tiles_u = (int)((g->n_u + p.ts.tu - 1) / p.ts.tu);
+        p.tiles_v = (int)((g->n_v + tile_v_extent - 1) / tile_v_extent);
+        p.row_words = fused_row_words(p.fb);
+        p.slab_bytes = ((int64_t)a->n_sample * p.fb * es + 15) / 16 * 16;
+        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+        size_t off = 0;
+        p.off_S = off;
+        off += al((size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes);
+        p.off_rxr = off;
+        off += al((size_t)g->n_ele * p.tiles_u * p.tiles_z * sizeof(float2));
+        p.off_txr = off;
+        off += al((size_t)g->n_tx * p.tiles_v * p.tiles_z * sizeof(float2));
+        p.total = off;
+        p.n_items = (int64_t)p.n_fb * p.tiles_z * p.tiles_u * p.tiles_v;
+    };
+
+    // Voxel-blocked kernel: exact tables, a steering axis to block along,
+    // frames in pairs, and at most 2 rows of shift inside a block.
+    const bool vb_fb_ok = fb_req == 0 ? a->n_frame >= 2 : (fb_req == 2 || fb_req == 4 || fb_req == 8);
+    if (g->mode == MODE_EXACT && vb_fb_ok && a->kernel != RCABF_KERNEL_FUSED_NOBLOCK) {
+        const int d = g->vb_shift(VB_BLOCK);
+        if (d >= 1 && d <= 2) {
+            const int tu = std::min(4, pow2_ceil(g->n_u));
+            const int tvb = 2;
+            const TileShape vts{tu, tvb, VB_THREADS_HOST / (tu * tvb)};
+            const int need = (int)std::min<int64_t>(
+                g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
+            int fb = 0;
+            for (int c : {8, 4, 2}) {
+                if (fb_req > 0 && c != fb_req) continue;
+                if (fb_req == 0 && c > 2 * a->n_frame) continue;
+                const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
+                                                                       fused_row_words(c) * 4)),
+                                              vb_stage_rows_cap(p.store, c));
+                if (cap >= need) { fb = c; break; }
+            }
+            if (fb) {
+                p.vb = 1;
+                p.d = d;
+                p.fb = fb;
+                p.ts = vts;
+                layout(vts.tv * VB_BLOCK);
+                p.wmax = need;
+                p.smem = vb_smem_bytes(p.store, p.wmax, p.row_words);
+                return RCABF_OK;
+            }
+        }
+    }
+
     p.ts = default_tile(g);
     // the largest window of any (tile, tx, rx) step, rounded up: the staging
     // buffers hold it, so the kernel never needs a fallback path
@@ -141,26 +194,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
         p.total = 0;
         return RCABF_OK;
     }
-    p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
-    p.tiles_z = (int)((g->n_z + p.ts.tz - 1) / p.ts.tz);
-    p.tiles_u = (int)((g->n_u + p.ts.tu - 1) / p.ts.tu);
-    p.tiles_v = (int)((g->n_v + p.ts.tv - 1) / p.ts.tv);
-    const int es = store_bytes(p.store);
-    const int rowb = p.fb * es;
-    p.row_words = fused_row_words(p.fb);
+    layout(p.ts.tv);
     p.wmax = std::max(kind_taps(g->kind), need);
     p.smem = fused_smem_bytes(g->mode, g->kind, p.store, p.wmax, p.row_words);
-    p.slab_bytes = ((int64_t)a->n_sample * rowb + 15) / 16 * 16;
-    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    size_t off = 0;
-    p.off_S = off;
-    off += al((size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes);
-    p.off_rxr = off;
-    off += al((size_t)g->n_ele * p.tiles_u * p.tiles_z * sizeof(float2));
-    p.off_txr = off;
-    off += al((size_t)g->n_tx * p.tiles_v * p.tiles_z * sizeof(float2));
-    p.total = off;
-    p.n_items = (int64_t)p.n_fb * p.tiles_z * p.tiles_u * p.tiles_v;
     return RCABF_OK;
 }
 
@@ -188,7 +224,7 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
     if ((ce = launch_range(rr, st)) != cudaSuccess) return cuda_fail(ce, "rx range launch");
     RangeParams tr = rr;
     tr.tab = g->tx_tab; tr.out = reinterpret_cast<float2 *>(ws + p.off_txr); tr.rows = g->n_tx;
-    tr.n_a = g->n_v; tr.ta = p.ts.tv; tr.tiles_a = p.tiles_v; tr.is_rx = 0;
+    tr.n_a = g->n_v; tr.ta = p.vb ? p.ts.tv * VB_BLOCK : p.ts.tv; tr.tiles_a = p.tiles_v; tr.is_rx = 0;
     if ((ce = launch_range(tr, st)) != cudaSuccess) return cuda_fail(ce, "tx range launch");
     g_launches += 3;
     if (marks) mark(marks, 2, st);
@@ -211,22 +247,27 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
 {
     DeviceState *ds = device_state(g0->device);
     prm.err_count = ds->err;
-    const size_t smem = fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
-    const std::array<int64_t, 5> key{g0->mode, g0->kind, p.fb, p.store, (int64_t)smem};
+    const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words)
+                             : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
+    // variant key: (mode or 2 + row shift for the voxel-blocked kernel, kind, fb, store, smem)
+    const std::array<int64_t, 5> key{p.vb ? 2 + p.d : g0->mode, g0->kind, p.fb, p.store, (int64_t)smem};
     int occ;
     {
         std::lock_guard<std::mutex> lk(ds->mu);
         if (!ds->prepared[key]) {
-            const cudaError_t pe = prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
+            const cudaError_t pe = p.vb ? prepare_fused_vb(g0->kind, p.d, p.fb, p.store, smem)
+                                        : prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
             if (pe != cudaSuccess) return cuda_fail(pe, "fused kernel shared-memory attribute");
             ds->prepared[key] = true;
-            ds->occ[key] = fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
+            ds->occ[key] = p.vb ? fused_vb_occupancy(g0->kind, p.d, p.fb, p.store, smem)
+                                : fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
         }
         occ = std::max(1, ds->occ[key]);
     }
     const int64_t grid = std::min<int64_t>(prm.n_items, (int64_t)ds->n_sm * occ);
     if (grid <= 0) return RCABF_OK;
-    const cudaError_t le = launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st);
+    const cudaError_t le = p.vb ? launch_fused_vb(g0->kind, p.d, p.fb, p.store, prm, (int)grid, smem, st)
+                                : launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st);
     if (le != cudaSuccess) return cuda_fail(le, "fused kernel launch");
     g_launches += 1;
     return RCABF_OK;
@@ -386,6 +427,22 @@ int rcabf_beamform_workspace_size(const rcabf_geometry *g, const rcabf_beamform_
     return s;
 }
 
+int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, char *buf, size_t len)
+{
+    if (!buf || len == 0) return RCABF_ERR_INVALID_ARGUMENT;
+    Plan p;
+    int s = plan_beamform(const_cast<rcabf_geometry *>(g), a, p);
+    if (s != RCABF_OK) return s;
+    const char *kname = p.kernel == RCABF_KERNEL_PLAIN ? "plain" : p.vb ? "fused_voxel_blocked" : "fused";
+    snprintf(buf, len,
+             "{\"kernel\": \"%s\", \"row_shift\": %d, \"frames_per_block\": %d, \"frame_blocks\": %d, "
+             "\"tile\": [%d, %d, %d], \"voxels_per_thread\": %d, \"window_rows\": %d, \"smem_bytes\": %zu, "
+             "\"workspace_bytes\": %zu, \"work_items\": %lld, \"storage\": %d}",
+             kname, p.d, p.fb, p.n_fb, p.ts.tu, p.vb ? p.ts.tv * VB_BLOCK : p.ts.tv, p.ts.tz, p.vb ? VB_BLOCK : 1,
+             p.wmax, p.smem, p.total, (long long)p.n_items, p.store);
+    return RCABF_OK;
+}
+
 int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream)
 {
     if (!g) return RCABF_ERR_BAD_HANDLE;
@@ -417,7 +474,8 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_bea
         if ((s = check_ptrs(&as[i], p)) != RCABF_OK) return s;
         if (i == 0) p0 = p;
         // one launch = one kernel variant: every job fused, same frame block
-        if (p.kernel != RCABF_KERNEL_FUSED || p.fb != p0.fb) return RCABF_ERR_UNSUPPORTED;
+        if (p.kernel != RCABF_KERNEL_FUSED || p.fb != p0.fb || p.vb != p0.vb || p.d != p0.d)
+            return RCABF_ERR_UNSUPPORTED;
         wmax = std::max(wmax, p.wmax);
         if ((s = stage_job(g, &as[i], p, prm.jobs[i], st)) != RCABF_OK) return s;
         prm.jobs[i].item_begin = items;

@@ -83,3 +83,54 @@ static cudaError_t plain_iq(const PlainParams &p, cudaStream_t st)
         return plain_iq<MODE_EXACT, KIND>(p, st);                                                   \
     }                                                                                               \
     }
+
+// ---- voxel-blocked kernel (fused_vb_kernel.cuh) ----
+#include "fused_vb_kernel.cuh"
+
+namespace rcabf {
+
+template <int KIND, int FB, int STORE, int D>
+static cudaError_t vb_do(const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
+{
+    auto k = fused_vb_kernel<KIND, FB, STORE, D>;
+    if (what == 1) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (what == 2) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, VB_THREADS, smem);
+    k<<<grid, VB_THREADS, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+template <int KIND, int STORE, int D>
+static cudaError_t vb_fb(int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
+{
+    switch (fb) {
+    case 2: return vb_do<KIND, 2, STORE, D>(p, grid, smem, st, what, occ);
+    case 4: return vb_do<KIND, 4, STORE, D>(p, grid, smem, st, what, occ);
+    case 8: return vb_do<KIND, 8, STORE, D>(p, grid, smem, st, what, occ);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int KIND, int D>
+static cudaError_t vb_store(int store, int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st,
+                            int what, int *occ)
+{
+    switch (store) {
+    case ST_F32: return vb_fb<KIND, ST_F32, D>(fb, p, grid, smem, st, what, occ);
+    case ST_F16: return vb_fb<KIND, ST_F16, D>(fb, p, grid, smem, st, what, occ);
+    case ST_BF16: return vb_fb<KIND, ST_BF16, D>(fb, p, grid, smem, st, what, occ);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace rcabf
+
+#define RCABF_VB_TU(KIND, NAME)                                                                      \
+    namespace rcabf {                                                                                \
+    cudaError_t vb_entry_##NAME(int d, int store, int fb, const FusedParams *p, int grid, size_t smem,\
+                                cudaStream_t st, int what, int *occ)                                 \
+    {                                                                                                \
+        if (d == 1) return vb_store<KIND, 1>(store, fb, p, grid, smem, st, what, occ);               \
+        if (d == 2) return vb_store<KIND, 2>(store, fb, p, grid, smem, st, what, occ);               \
+        return cudaErrorInvalidValue;                                                                \
+    }                                                                                                \
+    }

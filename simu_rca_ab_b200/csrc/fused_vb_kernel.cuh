@@ -1,0 +1,397 @@
+// Fused persistent delay-and-sum kernel with voxel blocking along the
+// transmit-steering axis (sm_100a, EXACT tables, rectilinear grids).
+//
+// Why: a warp-wide 16-byte shared-memory load is served per quarter warp,
+// i.e. it costs 4 L1 wavefronts whatever the addresses, so a thread that
+// owns one voxel feeds only 4 FMAs per 16 bytes loaded and the kernel cannot
+// pass ~25-30% of the FP32 pipe.  Here each thread owns VB = 4 voxels that
+// differ only in v (the transmit-steering coordinate): they share the
+// receive delay, apodisation and receive phasor, and their transmit delays
+// differ by less than D samples over the block (checked on the host for
+// the whole acquisition).  Per (tx, rx) step the thread loads the
+// TAPS + D sample rows that cover all four voxels once and applies each
+// voxel's weights shifted to its own first row (zeros elsewhere): one
+// 16-byte load (two frames) now feeds 16 FMAs.
+//
+// Tile: tu (receive axis) x tv*VB (steering axis) x tz (depth) voxels,
+// 128 threads; windows staged exactly as in fused_kernel.cuh (FP32 rows,
+// cp.async for complex64 slabs, register staging + conversion for FP16/
+// BF16).  The interpolation weights come from degree-8 polynomials
+// (weight_poly.h) on the FMA pipe, not from shared memory.
+#pragma once
+
+#include "das_common.cuh"
+#include "weight_poly.h"
+
+namespace rcabf {
+
+constexpr int VB = VB_BLOCK;
+constexpr int VB_THREADS = VB_THREADS_HOST;
+
+template <int FB, int BYTES> struct VbChunk;
+template <int FB> struct VbChunk<FB, 16> { using T = uint4; };
+template <int FB> struct VbChunk<FB, 8> { using T = uint2; };
+template <int FB> struct VbChunk<FB, 4> { using T = uint32_t; };
+
+__device__ __forceinline__ float2 packed16_to_f2(uint32_t b, int store)
+{
+    if (store == ST_F16) {
+        __half2 h;
+        memcpy(&h, &b, 4);
+        return __half22float2(h);
+    }
+    return make_float2(__uint_as_float(b << 16), __uint_as_float(b & 0xffff0000u));
+}
+
+// Weights w[0..TAPS) at fractional offset d in [0, 1).
+template <int KIND>
+__device__ __forceinline__ void poly_weights(float d, float (&w)[KindTraits<KIND>::TAPS])
+{
+    if constexpr (KIND == K_QUAD3) {
+        w[0] = 0.5f * d * (d - 1.0f);
+        w[1] = (1.0f - d) * (1.0f + d);
+        w[2] = 0.5f * d * (d + 1.0f);
+    } else {
+        using WP = WeightPoly<KIND>;
+        constexpr int T = KindTraits<KIND>::TAPS;
+        const float u = fmaf(2.0f, d, -1.0f);
+#pragma unroll
+        for (int j = 0; j < WP::HALF; ++j) {
+            float a = WP::c(j, WPOLY_DEG), b = WP::c(j, WPOLY_DEG);
+#pragma unroll
+            for (int m = WPOLY_DEG - 1; m >= 0; --m) {
+                a = fmaf(a, u, WP::c(j, m));
+                b = fmaf(b, -u, WP::c(j, m));
+            }
+            w[j] = a;
+            w[T - 1 - j] = b;
+        }
+    }
+}
+
+// Window of the tile for one step, extended by D rows past the last tap so
+// that every thread's TAPS + D rows are staged (rows beyond the record are
+// clamped; they carry zero weight).
+template <int KIND, int D>
+__device__ __forceinline__ Window vb_window(const FusedJob &J, int tx, int rx, int tu, int tv, int tz, float ab,
+                                            int wmax)
+{
+    using KT = KindTraits<KIND>;
+    Window w;
+    w.lo = 0; w.count = 0; w.overflow = false; w.skip = true;
+    const float2 rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
+    const float2 tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
+    if (!(rr.x <= rr.y) || !(tr.x <= tr.y)) return w;
+    float lo_f = __fadd_rn(__fadd_rn(tr.x, rr.x), ab);
+    float hi_f = __fadd_rn(__fadd_rn(tr.y, rr.y), ab);
+    const float fmax_n = (float)(J.n_sample);
+    lo_f = fminf(fmaxf(floorf(lo_f), -1.0f), fmax_n);
+    hi_f = fminf(fmaxf(floorf(hi_f), -1.0f), fmax_n);
+    int lo = (int)lo_f - KT::LO;
+    int hi_taps = (int)hi_f - KT::LO + KT::TAPS - 1;          // last tap row any voxel uses
+    lo = max(lo, 0);
+    if (min(hi_taps, J.n_sample - 2) < lo) return w;          // no usable sample in the window
+    const int hi = min(hi_taps + D, J.n_sample - 1);
+    w.skip = false;
+    w.lo = lo;
+    w.count = hi - lo + 1;
+    w.overflow = w.count > wmax;
+    return w;
+}
+
+template <int KIND, int FB, int STORE, int D>
+__global__ void __launch_bounds__(VB_THREADS)
+fused_vb_kernel(const __grid_constant__ FusedParams prm)
+{
+    static_assert(FB % 2 == 0, "frames are processed in pairs");
+    using T = typename StoreT<STORE>::T;
+    using KT = KindTraits<KIND>;
+    constexpr int TAPS = KT::TAPS;
+    constexpr int R = TAPS + D;                        // rows a thread reads per step
+    constexpr bool ASYNC = (STORE == ST_F32);
+    constexpr int NST = ASYNC ? 3 : 2;
+    constexpr int ES = (int)sizeof(T);
+    constexpr int RAWB = FB * ES;
+    constexpr int SROWB = FB * 8;
+    constexpr int CS = RAWB < 16 ? RAWB : 16;
+    constexpr int CPR = RAWB / CS;
+    constexpr int SREGS = VB_STAGE_REGS;               // staging chunks per thread (128 threads)
+    using Chunk = typename VbChunk<FB, CS>::T;
+
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int stride_s = prm.row_words * 4;
+    const int stage_bytes = prm.wmax * stride_s;
+    {
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (dyn < (unsigned)(NST * stage_bytes) || stride_s < SROWB ||
+            (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS)) {
+            if (tid == 0) atomicAdd(prm.err_count, 1ull);
+            return;
+        }
+    }
+    unsigned char *stages = smem;
+
+    for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x) {
+        int ji = 0;
+        while (ji + 1 < prm.n_jobs && prm.jobs[ji + 1].item_begin <= item) ++ji;
+        const FusedJob &J = prm.jobs[ji];
+        const DevGeom &g = J.g;
+        const int lu = tid % J.tu;
+        const int lvb = (tid / J.tu) % J.tv;
+        const int lz = tid / (J.tu * J.tv);
+        const int64_t local = item - J.item_begin;
+        const int64_t n_tiles = (int64_t)J.tiles_z * J.tiles_u * J.tiles_v;
+        const int fb = (int)(local / n_tiles);
+        const int64_t tile = local % n_tiles;
+        const int tz = (int)(tile % J.tiles_z);
+        const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
+        const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+        const int64_t iz = (int64_t)tz * J.tz + lz;
+        const int64_t iu = (int64_t)tu * J.tu + lu;
+        const int64_t iv0 = ((int64_t)tv * J.tv + lvb) * VB;
+        const bool zu = iz < g.n_z && iu < g.n_u;
+        const int64_t rem = g.n_v - iv0;
+        const int nvv = !zu ? 0 : rem <= 0 ? 0 : rem >= VB ? VB : (int)rem;
+        const int64_t rxkey = iu * g.n_z + iz;
+        const int64_t n_rxkey = g.n_u * g.n_z;
+        const int64_t n_txkey = g.n_v * g.n_z;
+        const int n_steps = g.n_tx * g.n_ele;
+        const char *S = reinterpret_cast<const char *>(J.S);
+
+        float2 acc[VB][FB];
+#pragma unroll
+        for (int v = 0; v < VB; ++v)
+#pragma unroll
+            for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
+
+        auto slab = [&](int tx, int rx) -> const char * {
+            return S + (((int64_t)tx * g.n_ele + rx) * J.n_fb + fb) * J.slab_bytes;
+        };
+        auto window = [&](int s) -> Window {
+            Window w;
+            w.skip = true; w.lo = 0; w.count = 0; w.overflow = false;
+            if (s >= n_steps) return w;
+            const int tx = s / g.n_ele, rx = s % g.n_ele;
+            return vb_window<KIND, D>(J, tx, rx, tu, tv, tz, ab_value(g, tx, rx), prm.wmax);
+        };
+        auto issue_async = [&](int s, const Window &w) {
+            if (!w.skip && !w.overflow) {
+                const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
+                unsigned char *dst = stages + (s % NST) * stage_bytes;
+                const int nch = w.count * CPR;
+                for (int c = tid; c < nch; c += VB_THREADS) {
+                    const int r = c / CPR, q = c % CPR;
+                    cp_async<CS>(dst + r * stride_s + q * CS, src + (int64_t)r * RAWB + q * CS);
+                }
+            }
+            cp_async_commit();
+        };
+        Chunk regs[SREGS];
+        auto load_regs = [&](int s, const Window &w) {
+            if (w.skip || w.overflow) return;
+            const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
+            const int nch = w.count * CPR;
+#pragma unroll
+            for (int k = 0; k < SREGS; ++k) {
+                const int c = tid + k * VB_THREADS;
+                if (c < nch) regs[k] = __ldg(reinterpret_cast<const Chunk *>(src + (int64_t)c * CS));
+            }
+        };
+        auto store_regs = [&](int s, const Window &w) {
+            if (w.skip || w.overflow) return;
+            unsigned char *dst = stages + (s % NST) * stage_bytes;
+            const int nch = w.count * CPR;
+#pragma unroll
+            for (int k = 0; k < SREGS; ++k) {
+                const int c = tid + k * VB_THREADS;
+                if (c < nch) {
+                    const int r = c / CPR, q = c % CPR;
+                    float2 *o = reinterpret_cast<float2 *>(dst + r * stride_s + q * CS * 2);
+                    uint32_t b[CS / 4];
+                    memcpy(b, &regs[k], CS);
+#pragma unroll
+                    for (int v = 0; v < CS / 4; v += 2) {
+                        if (v + 1 < CS / 4) {
+                            const float2 x0 = packed16_to_f2(b[v], STORE), x1 = packed16_to_f2(b[v + 1], STORE);
+                            *reinterpret_cast<float4 *>(o + v) = make_float4(x0.x, x0.y, x1.x, x1.y);
+                        } else {
+                            o[v] = packed16_to_f2(b[v], STORE);
+                        }
+                    }
+                }
+            }
+        };
+
+        Window wA = window(0), wB = window(1), wC;
+        if constexpr (ASYNC) {
+            issue_async(0, wA);
+            issue_async(1, wB);
+        } else {
+            load_regs(0, wA);
+            store_regs(0, wA);
+            load_regs(1, wB);
+            __syncthreads();
+        }
+
+        // per-transmit state of the thread's voxels: index part, phasor, cone
+        float txi[VB], txr[VB], txq[VB];
+        unsigned cone_bits = 0;
+#pragma unroll
+        for (int v = 0; v < VB; ++v) { txi[v] = 0.f; txr[v] = 0.f; txq[v] = 0.f; }
+        float4 enext = nvv > 0 ? __ldg(&g.rx_tab[rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
+
+        for (int s = 0; s < n_steps; ++s) {
+            const int tx = s / g.n_ele, rx = s % g.n_ele;
+            if constexpr (ASYNC) {
+                cp_async_wait<NST - 2>();
+                __syncthreads();
+                wC = window(s + 2);
+                issue_async(s + 2, wC);
+            }
+            const float4 e = enext;
+            if (nvv > 0 && s + 1 < n_steps)
+                enext = __ldg(&g.rx_tab[(int64_t)((s + 1) % g.n_ele) * n_rxkey + rxkey]);
+            if (rx == 0 && nvv > 0) {
+                cone_bits = 0;
+                const bool cu = g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
+#pragma unroll
+                for (int v = 0; v < VB; ++v) {
+                    if (v < nvv) {
+                        const float4 t = __ldg(&g.tx_tab[(int64_t)tx * n_txkey + (iv0 + v) * g.n_z + iz]);
+                        txi[v] = t.x; txr[v] = t.y; txq[v] = t.z;
+                        if (cu && t.w != 0.0f) cone_bits |= 1u << v;
+                    }
+                }
+            }
+
+            if (!wA.skip && cone_bits != 0 && e.w > 0.0f) {
+                const float ab = ab_value(g, tx, rx);
+                const float2 abp = ab_phasor(g, tx, rx);
+                // sample index of each voxel; rows are shared from the lowest
+                float fl[VB], dd[VB];
+                bool ok[VB];
+                float base = 3.0e38f;
+#pragma unroll
+                for (int v = 0; v < VB; ++v) {
+                    const float idx = __fadd_rn(__fadd_rn(txi[v], e.x), ab);
+                    fl[v] = floorf(idx);
+                    dd[v] = idx - fl[v];
+                    ok[v] = ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
+                            fl[v] < (float)(J.n_sample - 1 - KT::HI);
+                    if (ok[v]) base = fminf(base, fl[v]);
+                }
+                if (base < 2.0e38f) {
+                    float ws[VB][R];
+                    float2 P[VB];
+                    int omax = 0;
+#pragma unroll
+                    for (int v = 0; v < VB; ++v) {
+                        int o = (int)(fl[v] - base);
+                        if (ok[v] && o > D) { atomicAdd(prm.err_count, 1ull); ok[v] = false; }
+                        o = ok[v] ? o : 0;
+                        omax = max(omax, o);
+                        float w[TAPS];
+                        poly_weights<KIND>(dd[v], w);
+#pragma unroll
+                        for (int k = 0; k < R; ++k) {
+                            float a = (k < TAPS) ? w[k] : 0.0f;
+                            if constexpr (D >= 1) { if (o == 1) a = (k >= 1 && k - 1 < TAPS) ? w[k - 1] : 0.0f; }
+                            if constexpr (D >= 2) { if (o == 2) a = (k >= 2 && k - 2 < TAPS) ? w[k - 2] : 0.0f; }
+                            ws[v][k] = ok[v] ? a : 0.0f;
+                        }
+                        // P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab)
+                        const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
+                        P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
+                                     : make_float2(0.f, 0.f);
+                    }
+                    const int row0 = (int)base - KT::LO - wA.lo;
+                    if (row0 < 0 || row0 + TAPS + omax > wA.count || wA.overflow) {
+                        atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
+                    } else {
+                        const char *buf = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes;
+                        const int last = wA.count - 1;
+#pragma unroll
+                        for (int c = 0; c < FB; c += 2) {
+                            float4 ts[VB];
+#pragma unroll
+                            for (int v = 0; v < VB; ++v) ts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                            for (int k = 0; k < R; ++k) {
+                                const int row = min(row0 + k, last);
+                                const float4 x = *reinterpret_cast<const float4 *>(buf + row * stride_s + c * 8);
+#pragma unroll
+                                for (int v = 0; v < VB; ++v) {
+                                    ts[v].x = fmaf(ws[v][k], x.x, ts[v].x);
+                                    ts[v].y = fmaf(ws[v][k], x.y, ts[v].y);
+                                    ts[v].z = fmaf(ws[v][k], x.z, ts[v].z);
+                                    ts[v].w = fmaf(ws[v][k], x.w, ts[v].w);
+                                }
+                            }
+#pragma unroll
+                            for (int v = 0; v < VB; ++v) {
+                                float2 &a0 = acc[v][c], &a1 = acc[v][c + 1];
+                                a0.x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0.x));
+                                a0.y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0.y));
+                                a1.x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1.x));
+                                a1.y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1.y));
+                            }
+                        }
+                    }
+                }
+            }
+
+            if (rx == g.n_ele - 1 && !J.compound) {   // per-transmit output
+#pragma unroll
+                for (int v = 0; v < VB; ++v) {
+                    if (v < nvv) {
+                        const int64_t pix = iz * g.s_z + iu * g.s_u + (iv0 + v) * g.s_v;
+#pragma unroll
+                        for (int f = 0; f < FB; ++f) {
+                            const int fr = fb * FB + f;
+                            if (fr < J.n_frame) {
+                                float2 *o = J.out + ((int64_t)fr * g.n_tx + tx) * g.n_pix + pix;
+                                if (J.accumulate) { float2 q = *o; q.x += acc[v][f].x; q.y += acc[v][f].y; *o = q; }
+                                else *o = acc[v][f];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
+                }
+            }
+
+            if constexpr (!ASYNC) {
+                store_regs(s + 1, wB);
+                wC = window(s + 2);
+                load_regs(s + 2, wC);
+                __syncthreads();
+            }
+            wA = wB;
+            wB = wC;
+        }
+        if constexpr (ASYNC) cp_async_wait<0>();
+        __syncthreads();
+
+        if (J.compound) {
+#pragma unroll
+            for (int v = 0; v < VB; ++v) {
+                if (v < nvv) {
+                    const int64_t pix = iz * g.s_z + iu * g.s_u + (iv0 + v) * g.s_v;
+#pragma unroll
+                    for (int f = 0; f < FB; ++f) {
+                        const int fr = fb * FB + f;
+                        if (fr < J.n_frame) {
+                            float2 *o = J.out + (int64_t)fr * g.n_pix + pix;
+                            if (J.accumulate) { float2 q = *o; q.x += acc[v][f].x; q.y += acc[v][f].y; *o = q; }
+                            else *o = acc[v][f];
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+}  // namespace rcabf

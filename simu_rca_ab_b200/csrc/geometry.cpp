@@ -488,3 +488,32 @@ int rcabf_geometry::window_rows(const rcabf::TileShape &ts)
         m = std::max(m, it->second.rx_spread[i] + it->second.tx_spread[i]);
     return (int)std::ceil(m) + rcabf::kind_taps(kind) + 3;
 }
+
+int rcabf_geometry::vb_shift(int block)
+{
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = vb_shifts.find(block);
+    if (it != vb_shifts.end()) return it->second;
+    int d = -1;
+    if (mode == rcabf::MODE_EXACT && grid_kind == RCABF_GRID_RECTILINEAR && n_v >= 2) {
+        // The voxels of a block share the receive part of the index (and the
+        // aberration shift), so floor(itx_v + r) - floor(itx_w + r) is at
+        // most ceil(|itx_v - itx_w|); a margin covers the float sums.
+        float spread = 0.f;
+        for (int64_t t = 0; t < n_tx; ++t)
+            for (int64_t v0 = 0; v0 < n_v; v0 += block)
+                for (int64_t z = 0; z < n_z; ++z) {
+                    float lo = INFINITY, hi = -INFINITY;
+                    for (int64_t v = v0; v < std::min(n_v, v0 + block); ++v) {
+                        const float x = tx_delay[(size_t)((t * n_v + v) * n_z + z)];
+                        lo = std::min(lo, x);
+                        hi = std::max(hi, x);
+                    }
+                    spread = std::max(spread, hi - lo);
+                }
+        d = (int)std::ceil(spread + 1e-3f);
+        if (d < 1) d = 1;
+    }
+    vb_shifts[block] = d;
+    return d;
+}

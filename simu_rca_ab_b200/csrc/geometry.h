@@ -69,6 +69,11 @@ struct rcabf_geometry {
     // (tx, ele) step: spread of the transmit delay + spread of the receive
     // delay inside the tile (in samples) + the taps + rounding slack.
     int window_rows(const rcabf::TileShape &ts);
+    // Largest difference of floor(sample index) between voxels of one
+    // aligned block of `block` consecutive v (same u, z, tx, rx), i.e. the
+    // row shift bound D of the voxel-blocked kernel; -1 if not applicable.
+    int vb_shift(int block);
+    std::map<int, int> vb_shifts;
 };
 
 namespace rcabf {

@@ -14,6 +14,8 @@ constexpr size_t SMEM_BUDGET = 110 * 1024;
 
 struct Plan {
     int kernel = 0;       // rcabf_kernel
+    int vb = 0;           // 1: voxel-blocked kernel (fused_vb_kernel.cuh)
+    int d = 0;            // its row shift bound
     int store = 0;
     int fb = 1, n_fb = 1;
     TileShape ts{1, 1, 256};
@@ -39,6 +41,18 @@ inline size_t fused_table_bytes(int mode, int kind) { return (mode == MODE_EXACT
 inline size_t fused_smem_bytes(int mode, int kind, int store, int wmax, int row_words)
 {
     return fused_table_bytes(mode, kind) + (size_t)fused_stages(store) * wmax * row_words * 4;
+}
+// The voxel-blocked kernel keeps no table; three CTAs of 128 threads share an SM.
+constexpr size_t VB_SMEM_BUDGET = 72 * 1024;
+inline size_t vb_smem_bytes(int store, int wmax, int row_words)
+{
+    return (size_t)fused_stages(store) * wmax * row_words * 4;
+}
+inline int vb_stage_rows_cap(int store, int fb)
+{
+    if (store == ST_F32) return 1 << 30;
+    const int rawb = fb * 4, cs = rawb < 16 ? rawb : 16;
+    return VB_STAGE_REGS * VB_THREADS_HOST / (rawb / cs);
 }
 // Staged rows are FP32 (8 bytes per frame), padded by 16 bytes when >= 16.
 inline int fused_row_words(int fb) { return fb * 8 >= 16 ? (fb * 8 + 16) / 4 : (fb * 8) / 4; }

@@ -91,6 +91,9 @@ struct FusedJob {
 constexpr int MAX_JOBS = 24;
 constexpr int FUSED_THREADS = 256;
 constexpr int FUSED_STAGES = 3;
+constexpr int VB_BLOCK = 4;          // voxels per thread along v in the voxel-blocked kernel
+constexpr int VB_THREADS_HOST = 128; // its CTA size
+constexpr int VB_STAGE_REGS = 2;     // 16-byte staging chunks a thread holds (FP16/BF16 slabs)
 
 struct FusedParams {
     FusedJob jobs[MAX_JOBS];

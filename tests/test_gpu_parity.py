@@ -151,13 +151,20 @@ def test_fused_equals_plain_and_frame_blocks(bf, c0_small, storage):
     directly instead of through the polyphase table: within 1e-4 (-80 dB)."""
     w, data, G, T, P, O = c0_small
     outs = {}
-    for fb in (1, 2, 4, 8, 16, 24, 32, 40):
-        outs[fb], _ = run(bf, data, G, T, P, O, kernel="fused", framesPerBlock=fb, storage=storage)
+    for kern in ("fused", "fused_noblock"):
+        for fb in (1, 2, 4, 8, 16, 24, 32, 40):
+            outs[(kern, fb)], _ = run(bf, data, G, T, P, O, kernel=kern, framesPerBlock=fb, storage=storage)
     plain, _ = run(bf, data, G, T, P, O, kernel="plain", storage=storage)
-    for fb, v in outs.items():
-        assert np.array_equal(v, outs[1]), fb
+    # one voxel per thread: table weights, identical bits for every frame block
+    for fb in (2, 4, 8, 16, 24, 32, 40):
+        assert np.array_equal(outs[("fused_noblock", fb)], outs[("fused_noblock", 1)]), fb
+    # voxel-blocked kernel (frame blocks 2, 4, 8): polynomial weights
+    for fb in (4, 8):
+        assert np.array_equal(outs[("fused", fb)], outs[("fused", 2)]), fb
+    assert H.rel_rms(outs[("fused", 8)], outs[("fused_noblock", 8)]) < 1e-4
     if storage == "float32":
-        assert H.rel_rms(outs[8], plain) < 1e-4, H.rel_rms(outs[8], plain)
+        assert H.rel_rms(outs[("fused", 8)], plain) < 1e-4, H.rel_rms(outs[("fused", 8)], plain)
+        assert H.rel_rms(outs[("fused_noblock", 8)], plain) < 1e-4
     assert _errcount() == 0
 
 
@@ -215,3 +222,60 @@ def test_bf_iq_rca_pmig_style(bf):
     iq = bf.BfIQRCA(raw, pmig)
     assert iq.shape == (24, 16, 2)
     assert np.isfinite(iq).all() and np.abs(iq).max() > 0
+
+
+# --------------------------------------------------------------------------
+# Full Doppler-ensemble geometry (96 x 96 x 160 voxels, 128 elements,
+# 11 transmits), 8 frames: the voxel-blocked kernel against the FP64 oracle
+# on random voxels, and against the one-voxel-per-thread kernel.
+# --------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def c2_small(cuda):
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c2", n_frame=8)
+    data = W.channel_data(w, seed=5, device="cuda")
+    return w, data
+
+
+def _beamform_dev(bf, w, data, storage, kernel):
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200.params import normalize
+    eng = bf.default_engine()
+    g0 = w.groups[0]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geom = eng.geometry(normalize(np.zeros(1, np.complex64), g0.Geometry, g0.Transmit, w.Param, w.Options))
+    code = {"float32": L.STORE_F32, "float16": L.STORE_F16, "bfloat16": L.STORE_BF16}[storage]
+    iq = data.contiguous() if storage != "float16" else data.contiguous().to(torch.complex32)
+    out = torch.empty((w.n_frame, 1, geom.n_pix), dtype=torch.complex64, device="cuda")
+    a = eng.make_args(geom, iq, iq_dtype=L.IQ_C32 if storage == "float16" else L.IQ_C64, n_sample=w.n_sample,
+                      n_frame=w.n_frame, out=out, mask=None, compound=True, storage=code,
+                      kernel={"fused": L.KERNEL_FUSED, "fused_noblock": L.KERNEL_FUSED_NOBLOCK}[kernel])
+    plan = eng.plan(geom, a)
+    eng.run(geom, a)
+    torch.cuda.synchronize()
+    return out[:, 0].cpu().numpy(), plan
+
+
+@pytest.mark.parametrize("storage,tol", [("float32", DB_FP32), ("float16", DB_FP16), ("bfloat16", DB_BF16)])
+def test_voxel_blocked_kernel_vs_fp64_on_c2_geometry(bf, c2_small, storage, tol):
+    from simu_rca_ab_b200 import workloads as W
+    w, data = c2_small
+    out, plan = _beamform_dev(bf, w, data, storage, "fused")
+    assert plan["kernel"] == "fused_voxel_blocked", plan
+    rng = np.random.default_rng(7)
+    pix = np.sort(rng.choice(out.shape[1], 1024, replace=False))
+    dn = data.cpu().numpy()
+    g0 = w.groups[0]
+    r = H.prepare(W.as_matlab(dn), g0.Geometry, g0.Transmit, w.Param, {"flagMaskTransmit": False})
+    f64, m64 = H.run_fp64(r, H.INTERP_LANCZOS, 4, data=dn, pix=pix)
+    c64, _ = H.compound(f64, m64, True)
+    rms, peak = H.error_db(out[:, pix], c64[:, 0])
+    print(f"voxel-blocked {storage} on c2 geometry: {rms:.1f} dB RMS, {peak:.1f} dB peak; plan {plan}")
+    assert rms <= tol
+    if storage == "float32":
+        ref, plan2 = _beamform_dev(bf, w, data, storage, "fused_noblock")
+        assert plan2["kernel"] == "fused"
+        assert H.rel_rms(out, ref) < 1e-4
+    assert _errcount() == 0
