@@ -34,8 +34,10 @@ struct DeviceState {
     unsigned long long *err = nullptr;
     int n_sm = 0;
     std::mutex mu;
-    std::map<std::array<int64_t, 5>, int> occ;   // (mode, kind, fb, store, smem) -> CTAs/SM
-    std::map<std::array<int64_t, 5>, bool> prepared;
+    std::map<std::array<int64_t, 5>, int> occ;        // (variant..., smem) -> CTAs/SM
+    // The dynamic shared-memory limit is an attribute of the kernel function,
+    // so it is only ever raised: variant -> largest limit set so far.
+    std::map<std::array<int64_t, 4>, size_t> smem_limit;
 };
 
 static std::mutex g_dev_mu;
@@ -249,20 +251,26 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     prm.err_count = ds->err;
     const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words)
                              : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
-    // variant key: (mode or 2 + row shift for the voxel-blocked kernel, kind, fb, store, smem)
-    const std::array<int64_t, 5> key{p.vb ? 2 + p.d : g0->mode, g0->kind, p.fb, p.store, (int64_t)smem};
+    // variant: (mode, or 2 + row shift for the voxel-blocked kernel; kind; fb; store)
+    const std::array<int64_t, 4> var{p.vb ? 2 + p.d : g0->mode, g0->kind, p.fb, p.store};
+    const std::array<int64_t, 5> key{var[0], var[1], var[2], var[3], (int64_t)smem};
     int occ;
     {
         std::lock_guard<std::mutex> lk(ds->mu);
-        if (!ds->prepared[key]) {
+        auto lim = ds->smem_limit.find(var);
+        if (lim == ds->smem_limit.end() || lim->second < smem) {
             const cudaError_t pe = p.vb ? prepare_fused_vb(g0->kind, p.d, p.fb, p.store, smem)
                                         : prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
             if (pe != cudaSuccess) return cuda_fail(pe, "fused kernel shared-memory attribute");
-            ds->prepared[key] = true;
-            ds->occ[key] = p.vb ? fused_vb_occupancy(g0->kind, p.d, p.fb, p.store, smem)
-                                : fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
+            ds->smem_limit[var] = smem;
         }
-        occ = std::max(1, ds->occ[key]);
+        auto oc = ds->occ.find(key);
+        if (oc == ds->occ.end()) {
+            const int o = p.vb ? fused_vb_occupancy(g0->kind, p.d, p.fb, p.store, smem)
+                               : fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
+            oc = ds->occ.emplace(key, o).first;
+        }
+        occ = std::max(1, oc->second);
     }
     const int64_t grid = std::min<int64_t>(prm.n_items, (int64_t)ds->n_sm * occ);
     if (grid <= 0) return RCABF_OK;

@@ -11,13 +11,16 @@
 // the whole acquisition).  Per (tx, rx) step the thread loads the
 // TAPS + D sample rows that cover all four voxels once and applies each
 // voxel's weights shifted to its own first row (zeros elsewhere): one
-// 16-byte load (two frames) now feeds 16 FMAs.
+// 16-byte load (two frames) feeds 16 FMAs.
 //
 // Tile: tu (receive axis) x tv*VB (steering axis) x tz (depth) voxels,
-// 128 threads; windows staged exactly as in fused_kernel.cuh (FP32 rows,
-// cp.async for complex64 slabs, register staging + conversion for FP16/
-// BF16).  The interpolation weights come from degree-8 polynomials
-// (weight_poly.h) on the FMA pipe, not from shared memory.
+// 128 threads; windows staged as FP32 rows of a compile-time stride
+// (FB * 8 + 16 bytes, so the loads use immediate offsets and 8 consecutive
+// rows hit distinct banks): cp.async for complex64 slabs, register staging
+// with one conversion for FP16/BF16 slabs.  Rows of the window past the end
+// of the record are zero-filled, so no load needs clamping.  The
+// interpolation weights come from degree-8 polynomials (weight_poly.h)
+// evaluated as (u, -u) pairs with packed FP32x2 FMAs.
 #pragma once
 
 #include "das_common.cuh"
@@ -55,30 +58,33 @@ __device__ __forceinline__ void poly_weights(float d, float (&w)[KindTraits<KIND
         using WP = WeightPoly<KIND>;
         constexpr int T = KindTraits<KIND>::TAPS;
         const float u = fmaf(2.0f, d, -1.0f);
+        const float2 uu = make_float2(u, -u);
 #pragma unroll
         for (int j = 0; j < WP::HALF; ++j) {
-            float a = WP::c(j, WPOLY_DEG), b = WP::c(j, WPOLY_DEG);
+            float2 a = WP::c2(j, WPOLY_DEG);
 #pragma unroll
-            for (int m = WPOLY_DEG - 1; m >= 0; --m) {
-                a = fmaf(a, u, WP::c(j, m));
-                b = fmaf(b, -u, WP::c(j, m));
-            }
-            w[j] = a;
-            w[T - 1 - j] = b;
+            for (int m = WPOLY_DEG - 1; m >= 0; --m) a = __ffma2_rn(a, uu, WP::c2(j, m));
+            w[j] = a.x;           // w_j(d)
+            w[T - 1 - j] = a.y;   // w_{T-1-j}(d) = w_j(1 - d)
         }
     }
 }
 
-// Window of the tile for one step, extended by D rows past the last tap so
-// that every thread's TAPS + D rows are staged (rows beyond the record are
-// clamped; they carry zero weight).
+// Window of the tile for one step: rows [lo, lo + count) cover every tap of
+// every voxel plus D rows of shift; the first `data` rows exist in the
+// record (the rest are zero-filled).
+struct VbWindow {
+    int lo, count, data;
+    bool skip, overflow;
+};
+
 template <int KIND, int D>
-__device__ __forceinline__ Window vb_window(const FusedJob &J, int tx, int rx, int tu, int tv, int tz, float ab,
-                                            int wmax)
+__device__ __forceinline__ VbWindow vb_window(const FusedJob &J, int tx, int rx, int tu, int tv, int tz, float ab,
+                                              int wmax)
 {
     using KT = KindTraits<KIND>;
-    Window w;
-    w.lo = 0; w.count = 0; w.overflow = false; w.skip = true;
+    VbWindow w;
+    w.lo = 0; w.count = 0; w.data = 0; w.overflow = false; w.skip = true;
     const float2 rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
     const float2 tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
     if (!(rr.x <= rr.y) || !(tr.x <= tr.y)) return w;
@@ -88,19 +94,20 @@ __device__ __forceinline__ Window vb_window(const FusedJob &J, int tx, int rx, i
     lo_f = fminf(fmaxf(floorf(lo_f), -1.0f), fmax_n);
     hi_f = fminf(fmaxf(floorf(hi_f), -1.0f), fmax_n);
     int lo = (int)lo_f - KT::LO;
-    int hi_taps = (int)hi_f - KT::LO + KT::TAPS - 1;          // last tap row any voxel uses
+    const int hi_taps = (int)hi_f - KT::LO + KT::TAPS - 1;   // last tap row any voxel uses
     lo = max(lo, 0);
-    if (min(hi_taps, J.n_sample - 2) < lo) return w;          // no usable sample in the window
-    const int hi = min(hi_taps + D, J.n_sample - 1);
+    if (min(hi_taps, J.n_sample - 2) < lo) return w;         // no usable sample in the window
+    const int hi = min(hi_taps, J.n_sample - 2) + D;         // + shift rows
     w.skip = false;
     w.lo = lo;
     w.count = hi - lo + 1;
+    w.data = min(hi, J.n_sample - 1) - lo + 1;
     w.overflow = w.count > wmax;
     return w;
 }
 
 template <int KIND, int FB, int STORE, int D>
-__global__ void __launch_bounds__(VB_THREADS)
+__global__ void __launch_bounds__(VB_THREADS, VB_MIN_BLOCKS)
 fused_vb_kernel(const __grid_constant__ FusedParams prm)
 {
     static_assert(FB % 2 == 0, "frames are processed in pairs");
@@ -113,19 +120,19 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
     constexpr int ES = (int)sizeof(T);
     constexpr int RAWB = FB * ES;
     constexpr int SROWB = FB * 8;
+    constexpr int STRIDE = SROWB + 16;                 // staged row stride (bytes)
     constexpr int CS = RAWB < 16 ? RAWB : 16;
     constexpr int CPR = RAWB / CS;
-    constexpr int SREGS = VB_STAGE_REGS;               // staging chunks per thread (128 threads)
+    constexpr int SREGS = VB_STAGE_REGS;               // staging chunks per thread
     using Chunk = typename VbChunk<FB, CS>::T;
 
     extern __shared__ __align__(16) unsigned char smem[];
     const int tid = threadIdx.x;
-    const int stride_s = prm.row_words * 4;
-    const int stage_bytes = prm.wmax * stride_s;
+    const int stage_bytes = prm.wmax * STRIDE;
     {
         unsigned dyn;
         asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-        if (dyn < (unsigned)(NST * stage_bytes) || stride_s < SROWB ||
+        if (dyn < (unsigned)(NST * stage_bytes) || prm.row_words * 4 != STRIDE ||
             (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS)) {
             if (tid == 0) atomicAdd(prm.err_count, 1ull);
             return;
@@ -169,46 +176,55 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         auto slab = [&](int tx, int rx) -> const char * {
             return S + (((int64_t)tx * g.n_ele + rx) * J.n_fb + fb) * J.slab_bytes;
         };
-        auto window = [&](int s) -> Window {
-            Window w;
-            w.skip = true; w.lo = 0; w.count = 0; w.overflow = false;
+        auto window = [&](int s) -> VbWindow {
+            VbWindow w;
+            w.skip = true; w.lo = 0; w.count = 0; w.data = 0; w.overflow = false;
             if (s >= n_steps) return w;
             const int tx = s / g.n_ele, rx = s % g.n_ele;
             return vb_window<KIND, D>(J, tx, rx, tu, tv, tz, ab_value(g, tx, rx), prm.wmax);
         };
-        auto issue_async = [&](int s, const Window &w) {
+        // rows [data, count) of a staged buffer hold zeros (shift rows past the record)
+        auto zero_tail = [&](unsigned char *dst, const VbWindow &w) {
+            const int nz = (w.count - w.data) * (SROWB / 16);
+            for (int c = tid; c < nz; c += VB_THREADS) {
+                const int r = w.data + c / (SROWB / 16), q = c % (SROWB / 16);
+                *reinterpret_cast<float4 *>(dst + r * STRIDE + q * 16) = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        };
+        auto issue_async = [&](int s, const VbWindow &w) {
             if (!w.skip && !w.overflow) {
                 const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
                 unsigned char *dst = stages + (s % NST) * stage_bytes;
-                const int nch = w.count * CPR;
+                const int nch = w.data * CPR;
                 for (int c = tid; c < nch; c += VB_THREADS) {
                     const int r = c / CPR, q = c % CPR;
-                    cp_async<CS>(dst + r * stride_s + q * CS, src + (int64_t)r * RAWB + q * CS);
+                    cp_async<CS>(dst + r * STRIDE + q * CS, src + (int64_t)r * RAWB + q * CS);
                 }
+                zero_tail(dst, w);
             }
             cp_async_commit();
         };
         Chunk regs[SREGS];
-        auto load_regs = [&](int s, const Window &w) {
+        auto load_regs = [&](int s, const VbWindow &w) {
             if (w.skip || w.overflow) return;
             const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
-            const int nch = w.count * CPR;
+            const int nch = w.data * CPR;
 #pragma unroll
             for (int k = 0; k < SREGS; ++k) {
                 const int c = tid + k * VB_THREADS;
                 if (c < nch) regs[k] = __ldg(reinterpret_cast<const Chunk *>(src + (int64_t)c * CS));
             }
         };
-        auto store_regs = [&](int s, const Window &w) {
+        auto store_regs = [&](int s, const VbWindow &w) {
             if (w.skip || w.overflow) return;
             unsigned char *dst = stages + (s % NST) * stage_bytes;
-            const int nch = w.count * CPR;
+            const int nch = w.data * CPR;
 #pragma unroll
             for (int k = 0; k < SREGS; ++k) {
                 const int c = tid + k * VB_THREADS;
                 if (c < nch) {
                     const int r = c / CPR, q = c % CPR;
-                    float2 *o = reinterpret_cast<float2 *>(dst + r * stride_s + q * CS * 2);
+                    float2 *o = reinterpret_cast<float2 *>(dst + r * STRIDE + q * CS * 2);
                     uint32_t b[CS / 4];
                     memcpy(b, &regs[k], CS);
 #pragma unroll
@@ -222,9 +238,10 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     }
                 }
             }
+            zero_tail(dst, w);
         };
 
-        Window wA = window(0), wB = window(1), wC;
+        VbWindow wA = window(0), wB = window(1), wC;
         if constexpr (ASYNC) {
             issue_async(0, wA);
             issue_async(1, wB);
@@ -235,11 +252,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             __syncthreads();
         }
 
-        // per-transmit state of the thread's voxels: index part, phasor, cone
-        float txi[VB], txr[VB], txq[VB];
         unsigned cone_bits = 0;
-#pragma unroll
-        for (int v = 0; v < VB; ++v) { txi[v] = 0.f; txr[v] = 0.f; txq[v] = 0.f; }
         float4 enext = nvv > 0 ? __ldg(&g.rx_tab[rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
 
         for (int s = 0; s < n_steps; ++s) {
@@ -253,29 +266,28 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             const float4 e = enext;
             if (nvv > 0 && s + 1 < n_steps)
                 enext = __ldg(&g.rx_tab[(int64_t)((s + 1) % g.n_ele) * n_rxkey + rxkey]);
+            const float4 *txrow = g.tx_tab + (int64_t)tx * n_txkey + iz;
             if (rx == 0 && nvv > 0) {
                 cone_bits = 0;
                 const bool cu = g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
 #pragma unroll
-                for (int v = 0; v < VB; ++v) {
-                    if (v < nvv) {
-                        const float4 t = __ldg(&g.tx_tab[(int64_t)tx * n_txkey + (iv0 + v) * g.n_z + iz]);
-                        txi[v] = t.x; txr[v] = t.y; txq[v] = t.z;
-                        if (cu && t.w != 0.0f) cone_bits |= 1u << v;
-                    }
-                }
+                for (int v = 0; v < VB; ++v)
+                    if (v < nvv && cu && __ldg(&txrow[(iv0 + v) * g.n_z]).w != 0.0f) cone_bits |= 1u << v;
             }
 
             if (!wA.skip && cone_bits != 0 && e.w > 0.0f) {
                 const float ab = ab_value(g, tx, rx);
                 const float2 abp = ab_phasor(g, tx, rx);
-                // sample index of each voxel; rows are shared from the lowest
+                // sample index of each voxel (transmit entries are L1-resident
+                // for the whole transmit); rows are shared from the lowest
+                float4 t[VB];
                 float fl[VB], dd[VB];
                 bool ok[VB];
                 float base = 3.0e38f;
 #pragma unroll
                 for (int v = 0; v < VB; ++v) {
-                    const float idx = __fadd_rn(__fadd_rn(txi[v], e.x), ab);
+                    t[v] = v < nvv ? __ldg(&txrow[(iv0 + v) * g.n_z]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float idx = __fadd_rn(__fadd_rn(t[v].x, e.x), ab);
                     fl[v] = floorf(idx);
                     dd[v] = idx - fl[v];
                     ok[v] = ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
@@ -302,16 +314,16 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                             ws[v][k] = ok[v] ? a : 0.0f;
                         }
                         // P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab)
-                        const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
+                        const float qx = fmaf(t[v].y, e.y, -t[v].z * e.z), qy = fmaf(t[v].y, e.z, t[v].z * e.y);
                         P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
                                      : make_float2(0.f, 0.f);
                     }
                     const int row0 = (int)base - KT::LO - wA.lo;
-                    if (row0 < 0 || row0 + TAPS + omax > wA.count || wA.overflow) {
+                    if (row0 < 0 || row0 + R > wA.count || wA.overflow) {
                         atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
                     } else {
-                        const char *buf = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes;
-                        const int last = wA.count - 1;
+                        const char *rows = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes +
+                                           row0 * STRIDE;
 #pragma unroll
                         for (int c = 0; c < FB; c += 2) {
                             float4 ts[VB];
@@ -319,8 +331,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                             for (int v = 0; v < VB; ++v) ts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                             for (int k = 0; k < R; ++k) {
-                                const int row = min(row0 + k, last);
-                                const float4 x = *reinterpret_cast<const float4 *>(buf + row * stride_s + c * 8);
+                                const float4 x = *reinterpret_cast<const float4 *>(rows + k * STRIDE + c * 8);
 #pragma unroll
                                 for (int v = 0; v < VB; ++v) {
                                     ts[v].x = fmaf(ws[v][k], x.x, ts[v].x);
@@ -338,6 +349,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                                 a1.y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1.y));
                             }
                         }
+                        (void)omax;
                     }
                 }
             }

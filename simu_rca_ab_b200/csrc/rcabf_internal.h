@@ -94,6 +94,7 @@ constexpr int FUSED_STAGES = 3;
 constexpr int VB_BLOCK = 4;          // voxels per thread along v in the voxel-blocked kernel
 constexpr int VB_THREADS_HOST = 128; // its CTA size
 constexpr int VB_STAGE_REGS = 2;     // 16-byte staging chunks a thread holds (FP16/BF16 slabs)
+constexpr int VB_MIN_BLOCKS = 1;     // launch-bounds hint: more forces spills (~230 registers live)
 
 struct FusedParams {
     FusedJob jobs[MAX_JOBS];
