@@ -155,7 +155,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
 
     // Voxel-blocked kernel: exact tables, a steering axis to block along,
     // frames in pairs, and at most 2 rows of shift inside a block.
-    const bool vb_fb_ok = fb_req == 0 ? a->n_frame >= 2 : (fb_req == 2 || fb_req == 4 || fb_req == 8);
+    const bool vb_fb_ok = fb_req == 0 ? a->n_frame >= 2 : (fb_req == 2 || fb_req == 4 || fb_req == 8 || fb_req == 16);
     if (g->mode == MODE_EXACT && vb_fb_ok && a->kernel != RCABF_KERNEL_FUSED_NOBLOCK) {
         const int d = g->vb_shift(VB_BLOCK);
         if (d >= 1 && d <= 2) {
@@ -165,7 +165,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
             const int need = (int)std::min<int64_t>(
                 g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
             int fb = 0;
-            for (int c : {8, 4, 2}) {
+            for (int c : {16, 8, 4, 2}) {
                 if (fb_req > 0 && c != fb_req) continue;
                 if (fb_req == 0 && c > 2 * a->n_frame) continue;
                 const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *

@@ -106,6 +106,7 @@ static cudaError_t vb_fb(int fb, const FusedParams *p, int grid, size_t smem, cu
     case 2: return vb_do<KIND, 2, STORE, D>(p, grid, smem, st, what, occ);
     case 4: return vb_do<KIND, 4, STORE, D>(p, grid, smem, st, what, occ);
     case 8: return vb_do<KIND, 8, STORE, D>(p, grid, smem, st, what, occ);
+    case 16: return vb_do<KIND, 16, STORE, D>(p, grid, smem, st, what, occ);
     default: return cudaErrorInvalidValue;
     }
 }

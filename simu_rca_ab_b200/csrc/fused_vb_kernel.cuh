@@ -19,8 +19,8 @@
 // rows hit distinct banks): cp.async for complex64 slabs, register staging
 // with one conversion for FP16/BF16 slabs.  Rows of the window past the end
 // of the record are zero-filled, so no load needs clamping.  The
-// interpolation weights come from degree-8 polynomials (weight_poly.h)
-// evaluated as (u, -u) pairs with packed FP32x2 FMAs.
+// interpolation weights come from degree-8 polynomials (weight_poly.h),
+// each mirrored pair of taps from one even and one odd chain.
 #pragma once
 
 #include "das_common.cuh"
@@ -55,17 +55,24 @@ __device__ __forceinline__ void poly_weights(float d, float (&w)[KindTraits<KIND
         w[1] = (1.0f - d) * (1.0f + d);
         w[2] = 0.5f * d * (d + 1.0f);
     } else {
+        // w_j(u) = E_j(u^2) + u O_j(u^2) and w_{T-1-j}(u) = w_j(-u) = E_j - u O_j:
+        // both weights of a mirrored pair from one even and one odd Horner
+        // chain in s = u^2 (DEG + 1 FMAs per pair)
         using WP = WeightPoly<KIND>;
         constexpr int T = KindTraits<KIND>::TAPS;
+        static_assert(WPOLY_DEG % 2 == 0, "even degree");
         const float u = fmaf(2.0f, d, -1.0f);
-        const float2 uu = make_float2(u, -u);
+        const float s = u * u;
 #pragma unroll
         for (int j = 0; j < WP::HALF; ++j) {
-            float2 a = WP::c2(j, WPOLY_DEG);
+            float e = WP::c(j, WPOLY_DEG);
 #pragma unroll
-            for (int m = WPOLY_DEG - 1; m >= 0; --m) a = __ffma2_rn(a, uu, WP::c2(j, m));
-            w[j] = a.x;           // w_j(d)
-            w[T - 1 - j] = a.y;   // w_{T-1-j}(d) = w_j(1 - d)
+            for (int m = WPOLY_DEG - 2; m >= 0; m -= 2) e = fmaf(e, s, WP::c(j, m));
+            float o = WP::c(j, WPOLY_DEG - 1);
+#pragma unroll
+            for (int m = WPOLY_DEG - 3; m >= 1; m -= 2) o = fmaf(o, s, WP::c(j, m));
+            w[j] = fmaf(u, o, e);             // w_j(d)
+            w[T - 1 - j] = fmaf(-u, o, e);    // w_{T-1-j}(d) = w_j(1 - d)
         }
     }
 }
@@ -252,7 +259,11 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             __syncthreads();
         }
 
+        // per-transmit state of the thread's voxels: index part, phasor, cone
+        float txi[VB], txr[VB], txq[VB];
         unsigned cone_bits = 0;
+#pragma unroll
+        for (int v = 0; v < VB; ++v) { txi[v] = 0.f; txr[v] = 0.f; txq[v] = 0.f; }
         float4 enext = nvv > 0 ? __ldg(&g.rx_tab[rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
 
         for (int s = 0; s < n_steps; ++s) {
@@ -266,28 +277,30 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             const float4 e = enext;
             if (nvv > 0 && s + 1 < n_steps)
                 enext = __ldg(&g.rx_tab[(int64_t)((s + 1) % g.n_ele) * n_rxkey + rxkey]);
-            const float4 *txrow = g.tx_tab + (int64_t)tx * n_txkey + iz;
             if (rx == 0 && nvv > 0) {
+                const float4 *txrow = g.tx_tab + (int64_t)tx * n_txkey + iz;
                 cone_bits = 0;
                 const bool cu = g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
 #pragma unroll
-                for (int v = 0; v < VB; ++v)
-                    if (v < nvv && cu && __ldg(&txrow[(iv0 + v) * g.n_z]).w != 0.0f) cone_bits |= 1u << v;
+                for (int v = 0; v < VB; ++v) {
+                    if (v < nvv) {
+                        const float4 t = __ldg(&txrow[(iv0 + v) * g.n_z]);
+                        txi[v] = t.x; txr[v] = t.y; txq[v] = t.z;
+                        if (cu && t.w != 0.0f) cone_bits |= 1u << v;
+                    }
+                }
             }
 
             if (!wA.skip && cone_bits != 0 && e.w > 0.0f) {
                 const float ab = ab_value(g, tx, rx);
                 const float2 abp = ab_phasor(g, tx, rx);
-                // sample index of each voxel (transmit entries are L1-resident
-                // for the whole transmit); rows are shared from the lowest
-                float4 t[VB];
+                // sample index of each voxel; rows are shared from the lowest
                 float fl[VB], dd[VB];
                 bool ok[VB];
                 float base = 3.0e38f;
 #pragma unroll
                 for (int v = 0; v < VB; ++v) {
-                    t[v] = v < nvv ? __ldg(&txrow[(iv0 + v) * g.n_z]) : make_float4(0.f, 0.f, 0.f, 0.f);
-                    const float idx = __fadd_rn(__fadd_rn(t[v].x, e.x), ab);
+                    const float idx = __fadd_rn(__fadd_rn(txi[v], e.x), ab);
                     fl[v] = floorf(idx);
                     dd[v] = idx - fl[v];
                     ok[v] = ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
@@ -314,7 +327,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                             ws[v][k] = ok[v] ? a : 0.0f;
                         }
                         // P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab)
-                        const float qx = fmaf(t[v].y, e.y, -t[v].z * e.z), qy = fmaf(t[v].y, e.z, t[v].z * e.y);
+                        const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
                         P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
                                      : make_float2(0.f, 0.f);
                     }

@@ -60,16 +60,9 @@ def main():
         out.append(f"// {name}: max fit error {err:.2e}")
         out.append(f"static __constant__ float WPOLY_{name}[{taps // 2}][{DEG + 1}] = {{")
         out.append("    " + ",\n    ".join(rows) + "};")
-        rows2 = []
-        for mono in coefs:
-            rows2.append("{" + ", ".join(f"{{{v:.9e}f, {v:.9e}f}}" for v in mono) + "}")
-        out.append(f"// the same coefficients duplicated, for paired (u, -u) evaluation")
-        out.append(f"static __constant__ float2 WPOLY2_{name}[{taps // 2}][{DEG + 1}] = {{")
-        out.append("    " + ",\n    ".join(rows2) + "};")
         out.append(f"template <> struct WeightPoly<{name}> {{")
         out.append(f"    static constexpr int HALF = {taps // 2};")
         out.append(f"    static __device__ __forceinline__ float c(int j, int m) {{ return WPOLY_{name}[j][m]; }}")
-        out.append(f"    static __device__ __forceinline__ float2 c2(int j, int m) {{ return WPOLY2_{name}[j][m]; }}")
         out.append("};")
         out.append("")
     out.append("}  // namespace rcabf")

@@ -62,7 +62,7 @@ cudaError_t prepare_fused(int mode, int kind, int fb, int store, size_t smem);
 int fused_occupancy(int mode, int kind, int fb, int store, size_t smem);
 
 // Voxel-blocked fused kernel (EXACT tables): d = row shift bound (1 or 2),
-// fb in {2, 4, 8}; 128 threads per CTA.
+// fb in {2, 4, 8, 16}; 128 threads per CTA.
 cudaError_t launch_fused_vb(int kind, int d, int fb, int store, const FusedParams &p, int grid, size_t smem,
                             cudaStream_t st);
 cudaError_t prepare_fused_vb(int kind, int d, int fb, int store, size_t smem);

@@ -158,8 +158,8 @@ def test_fused_equals_plain_and_frame_blocks(bf, c0_small, storage):
     # one voxel per thread: table weights, identical bits for every frame block
     for fb in (2, 4, 8, 16, 24, 32, 40):
         assert np.array_equal(outs[("fused_noblock", fb)], outs[("fused_noblock", 1)]), fb
-    # voxel-blocked kernel (frame blocks 2, 4, 8): polynomial weights
-    for fb in (4, 8):
+    # voxel-blocked kernel (frame blocks 2, 4, 8, 16): polynomial weights
+    for fb in (4, 8, 16):
         assert np.array_equal(outs[("fused", fb)], outs[("fused", 2)]), fb
     assert H.rel_rms(outs[("fused", 8)], outs[("fused_noblock", 8)]) < 1e-4
     if storage == "float32":
