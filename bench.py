@@ -40,6 +40,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "DAS voxel·rx·tx/s (nominal, summed over frames)"
 UNIT = "voxel·rx·tx/s"
+# plan kernel -> CUDA kernel function
+KERNEL_NAMES = {"fused_voxel_blocked": "fused_vb_kernel", "fused": "fused_das_kernel", "plain": "plain_das_kernel"}
 
 
 def parse():
@@ -56,6 +58,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-frame FP32 kernel comparison")
+    ap.add_argument("--plain-frames", type=int, default=10)
     ap.add_argument("--cpu-sample-frames", type=int, default=4)
     ap.add_argument("--cpu-sample-z", type=int, default=8)
     return ap.parse_args()
@@ -322,6 +326,35 @@ def main():
         e2e = {"value": units * world * a.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / a.steps}
 
+    # the plain one-launch-per-frame kernel on FP32 storage, complex64 input
+    # (the comparator of the fused path), timed on a sample of the frames
+    plain = None
+    if not a.no_plain and a.kernel != "plain":
+        pf = max(1, min(a.plain_frames, F))
+        p_in = [W.group_data(w, data[:pf], gi).contiguous() for gi in range(len(w.groups))]
+        p_out = torch.empty((pf, 1, n_pix), dtype=torch.complex64, device=dev)
+        p_args = [eng.make_args(g, p_in[gi], iq_dtype=L.IQ_C64, n_sample=w.n_sample, n_frame=pf, out=p_out,
+                                mask=None, compound=True, storage=L.STORE_F32, kernel=L.KERNEL_PLAIN,
+                                accumulate=gi > 0) for gi, g in enumerate(geoms)]
+
+        def plain_step():
+            for g, ar in zip(geoms, p_args):
+                eng.run(g, ar, stream=stream)
+
+        plain_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plain_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        p_ms = e0.elapsed_time(e1)
+        p_val = units / F * pf / (p_ms * 1e-3)
+        plain = {"value": p_val, "unit": UNIT, "frames": pf, "ms": p_ms,
+                 "kernel": "plain_das_kernel (one launch per frame, FP32 storage, complex64 input)",
+                 "ratio": (value / world) / p_val}
+        del p_in, p_out
+
     line = None
     if rank == 0:
         from oracle import host as H
@@ -341,7 +374,7 @@ def main():
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                 "frac": achieved / peak.value, "traffic": traffic,
                 "peak_source": "FP32 FMA probe kernel timed live in this run (MEASURED_PEAKS.json has no FP32 figure)",
-                "kernel": "fused_das_kernel", "kernel_ms": fused_ms,
+                "kernel": KERNEL_NAMES.get(plan.get("kernel"), plan.get("kernel")), "kernel_ms": fused_ms,
                 "work": f"{active:.4e} active units x {fpu} FLOP ({active / (units):.3f} of nominal)",
                 "nominal_achieved": units * fpu / (fused_ms * 1e-3) / 1e12}
         acc = None
@@ -377,7 +410,7 @@ def main():
                        "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)",
                        "plan": plan},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e,
+            "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
