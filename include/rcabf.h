@@ -232,6 +232,23 @@ int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *
 int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beamform_args *a,
                          void *stream);
 
+/* Size of the static device workspace of rcabf_beamform_noalloc (64 MiB). */
+#define RCABF_NOALLOC_WORKSPACE_BYTES ((size_t)64 << 20)
+
+/* rcabf_beamform through the fused kernel with a workspace that is a static
+ * device array of RCABF_NOALLOC_WORKSPACE_BYTES instead of a caller buffer
+ * (a->workspace and a->workspace_bytes are ignored): the call allocates no
+ * device memory.  No counterpart in the reference (its MEX gateway allocates
+ * per call).  The first call on each device looks up the static array's
+ * address with that device current and clears the array's error counter (a
+ * synchronous step): make it before any stream capture.  Rejected with
+ * RCABF_ERR_WORKSPACE_TOO_SMALL (detail in rcabf_last_error()) when the plan
+ * needs more than RCABF_NOALLOC_WORKSPACE_BYTES, and with
+ * RCABF_ERR_UNSUPPORTED when the plan is the plain kernel.  All calls on one
+ * device share the array: calls that overlap in time (other streams, other
+ * threads) race and must be serialised by the caller. */
+int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream);
+
 /* Count of device-side bound-check trips since the last call (expected 0). */
 int rcabf_take_error_count(int64_t *count);
 

@@ -78,6 +78,7 @@ _SIGS = {
     "rcabf_beamform": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_describe_plan": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_char_p, C.c_size_t]),
     "rcabf_beamform_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(BeamformArgs), C.c_void_p]),
+    "rcabf_beamform_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_measure_fp32_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),

@@ -43,16 +43,24 @@ struct DeviceState {
 static std::mutex g_dev_mu;
 static std::map<int, DeviceState *> g_dev;
 
-DeviceState *device_state(int dev)
+// with_err: also allocate the device error counter if it does not exist yet
+// (rcabf_beamform_noalloc asks for the host-side state only).
+DeviceState *device_state(int dev, bool with_err = true)
 {
     std::lock_guard<std::mutex> lk(g_dev_mu);
     auto it = g_dev.find(dev);
-    if (it != g_dev.end()) return it->second;
-    DeviceState *s = new DeviceState();
-    cudaDeviceGetAttribute(&s->n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaMalloc(&s->err, sizeof(unsigned long long)) != cudaSuccess) s->err = nullptr;
-    else cudaMemset(s->err, 0, sizeof(unsigned long long));
-    g_dev[dev] = s;
+    DeviceState *s;
+    if (it != g_dev.end()) {
+        s = it->second;
+    } else {
+        s = new DeviceState();
+        cudaDeviceGetAttribute(&s->n_sm, cudaDevAttrMultiProcessorCount, dev);
+        g_dev[dev] = s;
+    }
+    if (with_err && !s->err) {
+        if (cudaMalloc(&s->err, sizeof(unsigned long long)) != cudaSuccess) s->err = nullptr;
+        else cudaMemset(s->err, 0, sizeof(unsigned long long));
+    }
     return s;
 }
 
@@ -247,8 +255,9 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
 
 int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaStream_t st)
 {
-    DeviceState *ds = device_state(g0->device);
-    prm.err_count = ds->err;
+    // a counter set by the caller (rcabf_beamform_noalloc) is kept
+    DeviceState *ds = device_state(g0->device, prm.err_count == nullptr);
+    if (!prm.err_count) prm.err_count = ds->err;
     const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words)
                              : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
     // variant: (mode, or 2 + row shift for the voxel-blocked kernel; kind; fb; store)
@@ -331,6 +340,80 @@ int beamform_one(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t s
         g_launches += 1;
     }
     mark(a, 4, st);
+    return RCABF_OK;
+}
+
+// Static workspace of rcabf_beamform_noalloc, per device: looked up once with
+// the device current, its error counter cleared then.
+struct NoallocRegion {
+    void *ws = nullptr;
+    unsigned long long *err = nullptr;
+};
+static std::mutex g_noalloc_mu;
+static std::map<int, NoallocRegion> g_noalloc;
+
+static int noalloc_setup(int dev, NoallocRegion &r, bool create)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    auto it = g_noalloc.find(dev);
+    if (it != g_noalloc.end()) { r = it->second; return RCABF_OK; }
+    if (!create) return RCABF_ERR_PENDING;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return cuda_fail(e, "noalloc set-up: cudaGetDevice");
+    if (cur != dev) {
+        snprintf(g_last_err, sizeof(g_last_err),
+                 "noalloc set-up: the geometry's device %d is not the current device %d", dev, cur);
+        return RCABF_ERR_INVALID_ARGUMENT;
+    }
+    NoallocRegion n;
+    if ((e = noalloc_region(&n.ws, &n.err)) != cudaSuccess) return cuda_fail(e, "noalloc set-up: cudaGetSymbolAddress");
+    if ((e = cudaMemset(n.err, 0, sizeof(unsigned long long))) != cudaSuccess)
+        return cuda_fail(e, "noalloc set-up: clearing the error counter");
+    g_noalloc[dev] = n;
+    r = n;
+    return RCABF_OK;
+}
+
+int beamform_noalloc(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t st)
+{
+    if (!a) return RCABF_ERR_INVALID_ARGUMENT;
+    Plan p;
+    int s = plan_beamform(g, a, p);
+    if (s != RCABF_OK) return s;
+    if (p.kernel != RCABF_KERNEL_FUSED) {
+        snprintf(g_last_err, sizeof(g_last_err), "noalloc: the plan is the plain kernel; this entry runs the fused kernel only");
+        return RCABF_ERR_UNSUPPORTED;
+    }
+    if (p.total > RCABF_NOALLOC_WORKSPACE_BYTES) {
+        snprintf(g_last_err, sizeof(g_last_err),
+                 "noalloc: the plan needs %zu workspace bytes; the static workspace holds %zu", p.total,
+                 (size_t)RCABF_NOALLOC_WORKSPACE_BYTES);
+        return RCABF_ERR_WORKSPACE_TOO_SMALL;
+    }
+    NoallocRegion r;
+    if ((s = noalloc_setup(g->device, r, true)) != RCABF_OK) return s;
+    rcabf_beamform_args b = *a;
+    b.workspace = r.ws;
+    b.workspace_bytes = RCABF_NOALLOC_WORKSPACE_BYTES;
+    if ((s = check_ptrs(&b, p)) != RCABF_OK) return s;
+    mark(&b, 0, st);
+    FusedParams prm{};
+    if ((s = stage_job(g, &b, p, prm.jobs[0], st, &b)) != RCABF_OK) return s;
+    prm.jobs[0].item_begin = 0;
+    prm.n_jobs = 1;
+    prm.wmax = p.wmax;
+    prm.row_words = p.row_words;
+    prm.n_items = p.n_items;
+    prm.err_count = r.err;
+    if ((s = launch_fused_jobs(g, prm, p, st)) != RCABF_OK) return s;
+    mark(&b, 3, st);
+    if (b.mask) {
+        const cudaError_t me = launch_mask(g->dev(), b.mask, b.compound ? 1 : 0, b.accumulate ? 1 : 0, st);
+        if (me != cudaSuccess) return cuda_fail(me, "mask kernel launch");
+        g_launches += 1;
+    }
+    mark(&b, 4, st);
     return RCABF_OK;
 }
 
@@ -457,6 +540,12 @@ int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *
     return beamform_one(const_cast<rcabf_geometry *>(g), a, (cudaStream_t)stream);
 }
 
+int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    return beamform_noalloc(const_cast<rcabf_geometry *>(g), a, (cudaStream_t)stream);
+}
+
 int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_beamform_args *as, void *stream)
 {
     if (n < 1 || n > MAX_JOBS || !gs || !as) return RCABF_ERR_INVALID_ARGUMENT;
@@ -514,6 +603,13 @@ int rcabf_take_error_count(int64_t *count)
     if (!ds->err) return RCABF_ERR_CUDA;
     if (cudaMemcpy(&h, ds->err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return RCABF_ERR_CUDA;
     if (cudaMemset(ds->err, 0, sizeof(h)) != cudaSuccess) return RCABF_ERR_CUDA;
+    NoallocRegion r;   // plus the static counter of rcabf_beamform_noalloc, once set up
+    if (noalloc_setup(dev, r, false) == RCABF_OK) {
+        unsigned long long h2 = 0;
+        if (cudaMemcpy(&h2, r.err, sizeof(h2), cudaMemcpyDeviceToHost) != cudaSuccess) return RCABF_ERR_CUDA;
+        if (cudaMemset(r.err, 0, sizeof(h2)) != cudaSuccess) return RCABF_ERR_CUDA;
+        h += h2;
+    }
     *count = (int64_t)h;
     return RCABF_OK;
 }

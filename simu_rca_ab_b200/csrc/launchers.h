@@ -71,4 +71,8 @@ int fused_vb_occupancy(int kind, int d, int fb, int store, size_t smem);
 // Plain kernel: one frame.
 cudaError_t launch_plain(int mode, int kind, const PlainParams &p, cudaStream_t st);
 
+// Device addresses, on the current device, of the static workspace
+// (RCABF_NOALLOC_WORKSPACE_BYTES) and error counter of rcabf_beamform_noalloc.
+cudaError_t noalloc_region(void **ws, unsigned long long **err);
+
 }  // namespace rcabf
