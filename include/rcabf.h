@@ -238,8 +238,14 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beam
 /* rcabf_beamform through the fused kernel with a workspace that is a static
  * device array of RCABF_NOALLOC_WORKSPACE_BYTES instead of a caller buffer
  * (a->workspace and a->workspace_bytes are ignored): the call allocates no
- * device memory.  No counterpart in the reference (its MEX gateway allocates
- * per call).  The first call on each device looks up the static array's
+ * device memory.  It is for callers that may not call cudaMalloc: an
+ * acquisition loop that must not stall (cudaMalloc can synchronise the
+ * device), a host framework that owns the device memory pool (MATLAB's
+ * gpuArray allocator, a caching allocator that must see every allocation),
+ * or a plugin with no allocator of its own.  The array is held by every GPU
+ * that loads the library until the process exits.  No counterpart in the
+ * reference, whose wrapper allocates its outputs per call.  The first call
+ * on each device looks up the static array's
  * address with that device current and clears the array's error counter (a
  * synchronous step): make it before any stream capture.  Rejected with
  * RCABF_ERR_WORKSPACE_TOO_SMALL (detail in rcabf_last_error()) when the plan

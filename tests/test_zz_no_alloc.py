@@ -1,6 +1,12 @@
 """rcabf_beamform_noalloc: the fused path with its workspace in a static device
 array (no allocation per call), through the C ABI, against rcabf_beamform.
 
+The entry point serves callers that may not call cudaMalloc (acquisition
+loops that must not stall on an allocation, hosts that own the device memory
+pool); these tests check that it gives the bits of the allocating entry point
+on two calls in a row (a stale workspace would show on the second) and that
+it rejects what it cannot hold.
+
 The file name sorts last so that the static region is exercised both in a
 fresh process (run alone) and after every other test of the suite.
 """
