@@ -85,18 +85,37 @@ struct VbWindow {
     bool skip, overflow;
 };
 
+// Table bounds one step's window is computed from; loaded a step before
+// they are needed, so the window computation does not wait on L2.
+struct VbRanges {
+    float2 rr, tr;   // receive / transmit table delay range of the tile
+    float ab;        // aberration delay of the step
+};
+
+__device__ __forceinline__ VbRanges vb_ranges(const FusedJob &J, int s, int n_steps, int tu, int tv, int tz)
+{
+    VbRanges r;
+    if (s >= n_steps) {   // past the last step: an empty range (skipped)
+        r.rr = make_float2(1.0f, 0.0f); r.tr = r.rr; r.ab = 0.0f;
+        return r;
+    }
+    const int tx = s / J.g.n_ele, rx = s % J.g.n_ele;
+    r.rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
+    r.tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
+    r.ab = ab_value(J.g, tx, rx);
+    return r;
+}
+
 template <int KIND, int D>
-__device__ __forceinline__ VbWindow vb_window(const FusedJob &J, int tx, int rx, int tu, int tv, int tz, float ab,
-                                              int wmax)
+__device__ __forceinline__ VbWindow vb_window(const FusedJob &J, const VbRanges &r, int wmax)
 {
     using KT = KindTraits<KIND>;
     VbWindow w;
     w.lo = 0; w.count = 0; w.data = 0; w.overflow = false; w.skip = true;
-    const float2 rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
-    const float2 tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
+    const float2 rr = r.rr, tr = r.tr;
     if (!(rr.x <= rr.y) || !(tr.x <= tr.y)) return w;
-    float lo_f = __fadd_rn(__fadd_rn(tr.x, rr.x), ab);
-    float hi_f = __fadd_rn(__fadd_rn(tr.y, rr.y), ab);
+    float lo_f = __fadd_rn(__fadd_rn(tr.x, rr.x), r.ab);
+    float hi_f = __fadd_rn(__fadd_rn(tr.y, rr.y), r.ab);
     const float fmax_n = (float)(J.n_sample);
     lo_f = fminf(fmaxf(floorf(lo_f), -1.0f), fmax_n);
     hi_f = fminf(fmaxf(floorf(hi_f), -1.0f), fmax_n);
@@ -187,8 +206,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             VbWindow w;
             w.skip = true; w.lo = 0; w.count = 0; w.data = 0; w.overflow = false;
             if (s >= n_steps) return w;
-            const int tx = s / g.n_ele, rx = s % g.n_ele;
-            return vb_window<KIND, D>(J, tx, rx, tu, tv, tz, ab_value(g, tx, rx), prm.wmax);
+            return vb_window<KIND, D>(J, vb_ranges(J, s, n_steps, tu, tv, tz), prm.wmax);
         };
         // rows [data, count) of a staged buffer hold zeros (shift rows past the record)
         auto zero_tail = [&](unsigned char *dst, const VbWindow &w) {
@@ -249,6 +267,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
 
         VbWindow wA = window(0), wB = window(1), wC;
+        VbRanges rnext = vb_ranges(J, 2, n_steps, tu, tv, tz);   // ranges of the step two ahead
         if constexpr (ASYNC) {
             issue_async(0, wA);
             issue_async(1, wB);
@@ -271,7 +290,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             if constexpr (ASYNC) {
                 cp_async_wait<NST - 2>();
                 __syncthreads();
-                wC = window(s + 2);
+                wC = vb_window<KIND, D>(J, rnext, prm.wmax);
+                rnext = vb_ranges(J, s + 3, n_steps, tu, tv, tz);
                 issue_async(s + 2, wC);
             }
             const float4 e = enext;
@@ -389,7 +409,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
 
             if constexpr (!ASYNC) {
                 store_regs(s + 1, wB);
-                wC = window(s + 2);
+                wC = vb_window<KIND, D>(J, rnext, prm.wmax);
+                rnext = vb_ranges(J, s + 3, n_steps, tu, tv, tz);
                 load_regs(s + 2, wC);
                 __syncthreads();
             }
