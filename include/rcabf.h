@@ -255,6 +255,61 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beam
  * threads) race and must be serialised by the caller. */
 int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Serving: continuous batching of requests on one device                    */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference, which beamforms one synchronous call at a
+ * time (RCA.m:664-711).  A server owns an HBM arena (the admission budget),
+ * a set of streams (launch slots) and a scheduler thread.  Requests name
+ * caller-owned device buffers and a geometry handle, which must stay valid
+ * until the request completes; their workspace comes from the arena.
+ * Requests are admitted in arrival order as slots and arena space free up;
+ * queued requests whose plans run the same kernel variant are fused into one
+ * persistent launch.  A request whose output or mask is written by a launch
+ * in flight, or by an earlier queued request, waits for it, so requests that
+ * accumulate into one buffer apply in arrival order. */
+typedef struct rcabf_server rcabf_server;
+
+typedef struct rcabf_server_config {
+    int32_t struct_size;          /* sizeof(rcabf_server_config) */
+    int32_t device;               /* CUDA device ordinal */
+    size_t hbm_budget_bytes;      /* workspace arena, allocated once at creation */
+    int32_t n_streams;            /* launch slots in flight at once (1..64) */
+    int32_t max_queue;            /* queued requests beyond which submit returns RCABF_ERR_BUSY */
+    int32_t max_batch;            /* requests fused into one launch (1..24) */
+    int32_t batch_window_us;      /* with the device idle, wait this long after an arrival for
+                                     more requests to fuse (0 = launch at once) */
+} rcabf_server_config;
+
+typedef struct rcabf_server_stats {
+    int32_t struct_size;          /* sizeof(rcabf_server_stats) */
+    int32_t reserved;
+    int64_t submitted, completed, rejected, launches, in_flight, queued;
+    double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;   /* submit -> completion, host clock */
+    double units_done;            /* nominal voxel.rx.tx.frame units of completed requests */
+    double busy_s;                /* time with at least one launch in flight */
+    double span_s;                /* first submit -> last completion */
+    size_t arena_bytes, arena_peak_bytes;
+} rcabf_server_stats;
+
+/* Creates a server: allocates the arena on cfg->device (RCABF_ERR_OOM_ADMISSION
+ * if it does not fit) and starts the scheduler thread. */
+int rcabf_server_create(const rcabf_server_config *cfg, rcabf_server **out);
+/* Queues one request (a copy of *a; its workspace fields are ignored) and
+ * returns its ticket without waiting.  RCABF_ERR_OOM_ADMISSION when the plan's
+ * workspace is larger than the whole arena, RCABF_ERR_BUSY when the queue is
+ * full, plus rcabf_beamform's argument errors. */
+int rcabf_server_submit(rcabf_server *s, const rcabf_geometry *g, const rcabf_beamform_args *a, uint64_t *ticket);
+/* RCABF_ERR_PENDING while the request runs; RCABF_OK once it is done, with its
+ * own status in *status (the ticket is then released). */
+int rcabf_server_poll(rcabf_server *s, uint64_t ticket, int *status);
+/* As poll, but waits up to timeout_s seconds; RCABF_ERR_TIMEOUT if the request
+ * is still running then. */
+int rcabf_server_wait_for(rcabf_server *s, uint64_t ticket, double timeout_s, int *status);
+int rcabf_server_get_stats(rcabf_server *s, rcabf_server_stats *st);
+/* Runs the queued requests to completion, then frees the arena and streams. */
+int rcabf_server_destroy(rcabf_server *s);
+
 /* Count of device-side bound-check trips since the last call (expected 0). */
 int rcabf_take_error_count(int64_t *count);
 

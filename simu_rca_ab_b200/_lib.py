@@ -23,6 +23,7 @@ KERNEL_AUTO, KERNEL_FUSED, KERNEL_PLAIN, KERNEL_FUSED_NOBLOCK = 0, 1, 2, 3
 OK = 0
 ERR_OOM_ADMISSION = 104
 ERR_TIMEOUT = 105
+ERR_BUSY = 110
 ERR_PENDING = 111
 
 _dp = C.POINTER(C.c_double)
@@ -64,6 +65,27 @@ class BeamformArgs(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32), ("device", C.c_int32),
+        ("hbm_budget_bytes", C.c_size_t),
+        ("n_streams", C.c_int32), ("max_queue", C.c_int32),
+        ("max_batch", C.c_int32), ("batch_window_us", C.c_int32),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32), ("reserved", C.c_int32),
+        ("submitted", C.c_int64), ("completed", C.c_int64), ("rejected", C.c_int64),
+        ("launches", C.c_int64), ("in_flight", C.c_int64), ("queued", C.c_int64),
+        ("p50_ms", C.c_double), ("p95_ms", C.c_double), ("p99_ms", C.c_double),
+        ("mean_ms", C.c_double), ("max_ms", C.c_double),
+        ("units_done", C.c_double), ("busy_s", C.c_double), ("span_s", C.c_double),
+        ("arena_bytes", C.c_size_t), ("arena_peak_bytes", C.c_size_t),
+    ]
+
+
 # Every symbol include/rcabf.h declares, with its ctypes signature.
 _SIGS = {
     "rcabf_status_string": (C.c_char_p, [C.c_int]),
@@ -79,6 +101,12 @@ _SIGS = {
     "rcabf_describe_plan": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_char_p, C.c_size_t]),
     "rcabf_beamform_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_beamform_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
+    "rcabf_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "rcabf_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(BeamformArgs), C.POINTER(C.c_uint64)]),
+    "rcabf_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
+    "rcabf_server_wait_for": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_int)]),
+    "rcabf_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "rcabf_server_destroy": (C.c_int, [C.c_void_p]),
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_measure_fp32_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),

@@ -42,27 +42,23 @@ def test_status_strings_carry_reference_identifiers():
 
 def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
-    fields_g = [f[0] for f in L.GeometryDesc._fields_]
-    fields_b = [f[0] for f in L.BeamformArgs._fields_]
+    structs = {"g": (L.GeometryDesc, "rcabf_geometry_desc"), "b": (L.BeamformArgs, "rcabf_beamform_args"),
+               "c": (L.ServerConfig, "rcabf_server_config"), "s": (L.ServerStats, "rcabf_server_stats")}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rcabf.h"', "int main(void){"]
-    lines.append('printf("G %zu\\n", sizeof(rcabf_geometry_desc));')
-    lines.append('printf("B %zu\\n", sizeof(rcabf_beamform_args));')
-    for f in fields_g:
-        lines.append(f'printf("g.{f} %zu\\n", offsetof(rcabf_geometry_desc, {f}));')
-    for f in fields_b:
-        lines.append(f'printf("b.{f} %zu\\n", offsetof(rcabf_beamform_args, {f}));')
+    for tag, (py, cname) in structs.items():
+        lines.append(f'printf("{tag} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{tag}.{f} %zu\\n", offsetof({cname}, {f}));')
     lines.append("return 0;}")
     src.write_text("\n".join(lines))
     exe = tmp_path / "sz"
     gcc = HOST_CXX.replace("g++", "gcc")
     subprocess.run([gcc, "-I", str(INCLUDE), str(src), "-o", str(exe)], check=True)
     out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
-    assert int(out["G"]) == C.sizeof(L.GeometryDesc)
-    assert int(out["B"]) == C.sizeof(L.BeamformArgs)
-    for f in fields_g:
-        assert int(out[f"g.{f}"]) == getattr(L.GeometryDesc, f).offset, f
-    for f in fields_b:
-        assert int(out[f"b.{f}"]) == getattr(L.BeamformArgs, f).offset, f
+    for tag, (py, cname) in structs.items():
+        assert int(out[tag]) == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(out[f"{tag}.{f}"]) == getattr(py, f).offset, (cname, f)
 
 
 def test_null_arguments_are_rejected_without_a_device():
@@ -71,3 +67,23 @@ def test_null_arguments_are_rejected_without_a_device():
     n = C.c_size_t()
     assert lib.rcabf_beamform_workspace_size(None, None, C.byref(n)) == 100
     assert lib.rcabf_destroy_geometry(None) == 108
+
+
+def test_server_argument_checks_need_no_device():
+    lib = L.lib()
+    cfg = L.ServerConfig()
+    cfg.struct_size = C.sizeof(L.ServerConfig)
+    cfg.hbm_budget_bytes = 1 << 20
+    cfg.n_streams, cfg.max_queue, cfg.max_batch = 0, 4, 4      # no launch slot
+    h = C.c_void_p()
+    assert lib.rcabf_server_create(C.byref(cfg), C.byref(h)) == 100
+    cfg.n_streams, cfg.max_batch = 2, 25                      # more jobs than one launch holds
+    assert lib.rcabf_server_create(C.byref(cfg), C.byref(h)) == 100
+    cfg.struct_size = 8
+    assert lib.rcabf_server_create(C.byref(cfg), C.byref(h)) == 100
+    t = C.c_uint64()
+    st = C.c_int()
+    assert lib.rcabf_server_submit(None, None, None, C.byref(t)) == 108
+    assert lib.rcabf_server_poll(None, 1, C.byref(st)) == 108
+    assert lib.rcabf_server_wait_for(None, 1, 0.0, C.byref(st)) == 108
+    assert lib.rcabf_server_destroy(None) == 108
