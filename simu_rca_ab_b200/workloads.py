@@ -10,7 +10,7 @@ sizes of the configurations this beamformer is measured on:
       f-number 1.2, Lanczos a = 4
   c2  Doppler ensemble: 11 row plane waves -5..5 deg, [768 x 128 x 11 x 200],
       FP16/BF16 storage, grid 96 x 96 x 160, f-number 1.2, Lanczos a = 4
-  c3  serving mix (see serving.py)
+  c3  serving mix: a seeded stream of requests of mixed sizes (serving_mix)
   c4  256+256 probe, 32 row + 32 column plane waves -12..12 deg,
       [2048 x 256 x 64 x 4] FP16, grid 256 x 256 x 384, f-number 1.0, Lanczos a = 4
 
@@ -163,6 +163,62 @@ def get(name: str, *, n_frame: int | None = None, grid_scale: float = 1.0) -> Wo
                "lanczosOrder": a}
     return Workload(name, ns, nf, n, Param, Options, groups, (nz, nx, ny), a,
                     storage="float16" if name in ("c2", "c4") else "float32", scatter=scat)
+
+
+# ---------------------------------------------------------------------------
+# c3: the serving mix
+# ---------------------------------------------------------------------------
+C3_GRIDS = [(64, 32, 32), (128, 64, 64), (160, 96, 96), (256, 128, 128)]   # (Nz, Nx, Ny)
+C3_TX = [1, 2, 4, 8, 16, 32]
+
+
+def c3_workload(probe: int, n_tx: int, grid: tuple, n_frame: int) -> Workload:
+    """One serving-mix acquisition: a 64+64 probe (the c0 physics) or a
+    128+128 probe (the c1 physics), n_tx row plane waves received on the
+    columns, the given grid over the probe's field of view, f-number 1.5 and
+    Lanczos a = 3 for every request, synthesis as c0 (200 scatterers)."""
+    if probe == 64:
+        pitch, f0, fs, ns, lat, z0, zs, span = 0.3e-3, 7.8e6, 15.6e6, 512, 19e-3, 5e-3, 20e-3, 8.0
+    elif probe == 128:
+        pitch, f0, fs, ns, lat, z0, zs, span = 0.2e-3, 7.8e6, 15.6e6, 1024, 25.4e-3, 5e-3, 25e-3, 10.0
+    else:
+        raise ValueError("probe is 64 or 128 elements per side")
+    nz, nx, ny = grid
+    X, Y, Z = make_grid(nx, ny, nz, lat, lat, z0, zs)
+    th = np.linspace(-span, span, n_tx) if n_tx > 1 else np.zeros(1)
+    g = _group(probe, pitch, True, th, X, Y, Z, 0)
+    Param = {"samplingFrequency": fs, "demodulationFrequency": f0, "speedOfSound": C_SOUND,
+             "startTime": -(2 * z0 / C_SOUND - 16 / fs), "fnumber": 1.5}
+    Options = {"flagCompounding": True, "flagMaskTransmit": False, "interpolation": "lanczos", "lanczosOrder": 3}
+    half = lat / 2
+    scat = {"n": 200, "x": (-half, half), "y": (-half, half), "z": (z0, z0 + zs)}
+    return Workload(f"c3-{probe}-{n_tx}tx-{nz}x{nx}x{ny}", ns, n_frame, probe, Param, Options, [g], (nz, nx, ny), 3,
+                    storage="float32", scatter=scat)
+
+
+@dataclass
+class ServeRequest:
+    probe: int
+    n_tx: int
+    grid: tuple
+    n_frame: int
+    storage: str          # "float32" | "float16"
+    arrival_s: float      # Poisson arrival time from the start of the stream
+
+
+def serving_mix(seed: int, n_requests: int, rate_hz: float, max_frames: int = 64) -> list:
+    """Seeded request stream: probe 64+64 or 128+128, 1-32 transmits, 1-64
+    frames, grids from 32x32x64 to 128x128x256, FP32 or FP16 storage,
+    exponential inter-arrival times at ``rate_hz``."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n_requests))
+    out = []
+    for k in range(n_requests):
+        out.append(ServeRequest(probe=int(rng.choice([64, 128])), n_tx=int(rng.choice(C3_TX)),
+                                grid=C3_GRIDS[int(rng.integers(len(C3_GRIDS)))],
+                                n_frame=int(rng.integers(1, max_frames + 1)),
+                                storage=str(rng.choice(["float32", "float16"])), arrival_s=float(t[k])))
+    return out
 
 
 # ---------------------------------------------------------------------------
