@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-frame FP32 kernel comparison")
     ap.add_argument("--no-serving", action="store_true", help="skip the c3 serving-mix measurement")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the step")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
@@ -394,6 +395,55 @@ def main():
     units = w.units()
     value = units * world * a.steps / (total_ms * 1e-3)
 
+    # the same step captured once in a CUDA graph (no stage events inside) and
+    # replayed: checked bit-identical to the eager step, then timed
+    graph = None
+    if not a.no_graph:
+        try:
+            step()
+            torch.cuda.synchronize()
+            eager_out = out.clone()
+            g_args = []
+            for ar in args:
+                c = L.BeamformArgs.from_buffer_copy(ar)
+                c.stage_events = None
+                g_args.append(c)
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(stream)
+            with torch.cuda.stream(side):
+                for g, ar, wsp in zip(geoms, g_args, ws):
+                    eng.run(g, ar, workspace=wsp)
+            stream.wait_stream(side)
+            torch.cuda.synchronize()
+            L.lib().rcabf_take_launch_count(C.byref(C.c_int64()))
+            cg = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(cg):
+                for g, ar, wsp in zip(geoms, g_args, ws):
+                    eng.run(g, ar, workspace=wsp)
+            per_step = C.c_int64()
+            L.lib().rcabf_take_launch_count(C.byref(per_step))
+            out.zero_()
+            cg.replay()
+            torch.cuda.synchronize()
+            same = bool(torch.equal(out, eager_out))
+            barrier()
+            g0e, g1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0e.record(stream)
+            for _ in range(a.steps):
+                cg.replay()
+            g1e.record(stream)
+            torch.cuda.synchronize()
+            g_ms = g0e.elapsed_time(g1e)
+            if pg:
+                tt = torch.tensor([g_ms], device=dev)
+                pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+                g_ms = tt.item()
+            graph = {"ms_per_step": g_ms / a.steps, "value": units * world * a.steps / (g_ms * 1e-3),
+                     "kernels_per_step": int(per_step.value), "identical_to_eager": same}
+            del cg
+        except Exception as ex:   # reported in the line, the eager number stands
+            graph = {"error": f"{type(ex).__name__}: {ex}"}
+
     # fused-kernel time per launch: stage events of a separate, synchronised step
     step()
     torch.cuda.synchronize()
@@ -527,7 +577,7 @@ def main():
                        "plan": plan},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
-            "serving": serving,
+            "serving": serving, "graph": graph,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

@@ -279,3 +279,44 @@ def test_voxel_blocked_kernel_vs_fp64_on_c2_geometry(bf, c2_small, storage, tol)
         assert plan2["kernel"] == "fused"
         assert H.rel_rms(out, ref) < 1e-4
     assert _errcount() == 0
+
+
+def test_cuda_graph_capture_replays_the_same_bits(bf, c2_small):
+    """The whole beamform call (ingest, window ranges, fused kernel, mask)
+    captured once in a CUDA graph and replayed gives the eager call's bits."""
+    import ctypes as C
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200.params import normalize
+    w, data = c2_small
+    eng = bf.default_engine()
+    g0 = w.groups[0]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geom = eng.geometry(normalize(np.zeros(1, np.complex64), g0.Geometry, g0.Transmit, w.Param, w.Options))
+    iq = data.contiguous().to(torch.complex32)
+    out = torch.empty((w.n_frame, 1, geom.n_pix), dtype=torch.complex64, device="cuda")
+    mask = torch.empty((1, geom.n_pix), dtype=torch.float32, device="cuda")
+    a = eng.make_args(geom, iq, iq_dtype=L.IQ_C32, n_sample=w.n_sample, n_frame=w.n_frame, out=out, mask=mask,
+                      compound=True, storage=L.STORE_F16)
+    ws = torch.empty(max(256, eng.workspace_bytes(geom, a)), dtype=torch.uint8, device="cuda")
+    eng.run(geom, a, workspace=ws)
+    torch.cuda.synchronize()
+    ref, ref_mask = out.clone(), mask.clone()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        eng.run(geom, a, workspace=ws)
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        eng.run(geom, a, workspace=ws)
+    out.zero_()
+    mask.zero_()
+    for _ in range(2):
+        g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref) and torch.equal(mask, ref_mask)
+    n = C.c_int64()
+    L.check(L.lib().rcabf_take_error_count(C.byref(n)))
+    assert n.value == 0
