@@ -310,6 +310,7 @@ def main():
     from simu_rca_ab_b200 import _lib as L
     from simu_rca_ab_b200 import beamformer as B
     from simu_rca_ab_b200 import workloads as W
+    from simu_rca_ab_b200.multi import max_over_ranks
     from simu_rca_ab_b200.params import normalize
 
     torch.cuda.set_device(local)
@@ -388,10 +389,7 @@ def main():
     L.lib().rcabf_take_launch_count(C.byref(launches))
     step_ms = [t_ev[k].elapsed_time(t_ev[k + 1]) for k in range(a.steps)]
     total_ms = t_ev[0].elapsed_time(t_ev[-1])
-    if pg:
-        tt = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        total_ms = tt.item()
+    total_ms = max_over_ranks(total_ms, dev)
     units = w.units()
     value = units * world * a.steps / (total_ms * 1e-3)
 
@@ -434,10 +432,7 @@ def main():
             g1e.record(stream)
             torch.cuda.synchronize()
             g_ms = g0e.elapsed_time(g1e)
-            if pg:
-                tt = torch.tensor([g_ms], device=dev)
-                pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-                g_ms = tt.item()
+            g_ms = max_over_ranks(g_ms, dev)
             graph = {"ms_per_step": g_ms / a.steps, "value": units * world * a.steps / (g_ms * 1e-3),
                      "kernels_per_step": int(per_step.value), "identical_to_eager": same}
             del cg
@@ -477,10 +472,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
-        if pg:
-            tt = torch.tensor([e2e_ms], device=dev)
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            e2e_ms = tt.item()
+        e2e_ms = max_over_ranks(e2e_ms, dev)
         e2e = {"value": units * world * a.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / a.steps}
 
