@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-frame FP32 kernel comparison")
     ap.add_argument("--no-serving", action="store_true", help="skip the c3 serving-mix measurement")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the step")
+    ap.add_argument("--no-autotune", action="store_true", help="use the planner's launch choice untimed")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
@@ -353,6 +354,11 @@ def main():
                            frames_per_block=a.frames_per_block)
         ar.stage_events = C.cast(ev_arr[gi], C.POINTER(C.c_void_p))
         args.append(ar)
+    tune = None
+    if not a.no_autotune and kern == L.KERNEL_FUSED and a.frames_per_block == 0:
+        # launch choice (tile shape, window depth, frame block, kernel family)
+        # measured on this workload before the timed region
+        tune = [eng.autotune(g, ar, iters=1) for g, ar in zip(geoms, args)]
     ws = [torch.empty(max(256, eng.workspace_bytes(g, ar)), dtype=torch.uint8, device=dev)
           for g, ar in zip(geoms, args)]
     plan = eng.plan(geoms[0], args[0])
@@ -566,7 +572,7 @@ def main():
                                    f"f-number {w.Param['fnumber']}",
                        "storage": storage, "kernel": a.kernel, "l2": "inputs larger than L2 (no flush needed)",
                        "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)",
-                       "plan": plan},
+                       "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
             "serving": serving, "graph": graph,

@@ -255,6 +255,27 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beam
  * threads) race and must be serialised by the caller. */
 int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream);
 
+/* What rcabf_autotune chose for a geometry, frame count and storage. */
+typedef struct rcabf_tune_result {
+    int32_t struct_size;          /* sizeof(rcabf_tune_result) */
+    int32_t voxel_blocked;        /* 1: the voxel-blocked kernel, 0: one voxel per thread */
+    int32_t frames_per_block;
+    int32_t tile_u, tile_v, tile_z;   /* voxels per tile along the receive axis, steering axis, depth */
+    int32_t window_rows;          /* sample rows staged per step (the shared-memory window depth) */
+    int32_t candidates;           /* launch choices timed */
+    double best_ms, default_ms;   /* per call: the chosen one, the planner's own */
+} rcabf_tune_result;
+
+/* Times the fused kernel's launch choices (tile shape, hence window depth,
+ * frame block, kernel family) on these arguments and keeps the fastest for
+ * this geometry, frame count and storage: later calls with
+ * frames_per_block = 0 (or the chosen block) plan with it.  No counterpart
+ * in the reference, whose launch shape is fixed (RCA.m:640-650).
+ * Synchronous; allocates its own scratch; overwrites a->out (a->mask and
+ * a->accumulate are ignored).  iters: timed calls per candidate (1..100). */
+int rcabf_autotune(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream, int iters,
+                   rcabf_tune_result *res);
+
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching of requests on one device                    */
 /* ------------------------------------------------------------------------ */

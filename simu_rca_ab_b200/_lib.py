@@ -65,6 +65,15 @@ class BeamformArgs(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32), ("voxel_blocked", C.c_int32), ("frames_per_block", C.c_int32),
+        ("tile_u", C.c_int32), ("tile_v", C.c_int32), ("tile_z", C.c_int32),
+        ("window_rows", C.c_int32), ("candidates", C.c_int32),
+        ("best_ms", C.c_double), ("default_ms", C.c_double),
+    ]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [
         ("struct_size", C.c_int32), ("device", C.c_int32),
@@ -101,6 +110,8 @@ _SIGS = {
     "rcabf_describe_plan": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_char_p, C.c_size_t]),
     "rcabf_beamform_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_beamform_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
+    "rcabf_autotune": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p, C.c_int,
+                                 C.POINTER(TuneResult)]),
     "rcabf_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "rcabf_server_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(BeamformArgs), C.POINTER(C.c_uint64)]),
     "rcabf_server_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),

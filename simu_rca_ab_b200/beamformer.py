@@ -215,6 +215,17 @@ class Engine:
         L.check(L.lib().rcabf_describe_plan(C.c_void_p(geom.ptr), C.byref(a), buf, 1024), "rcabf_describe_plan")
         return json.loads(buf.value.decode())
 
+    def autotune(self, geom: GeometryHandle, a: L.BeamformArgs, iters: int = 1, stream=None) -> dict:
+        """Times the fused kernel's launch choices on these arguments and keeps
+        the fastest for this geometry, frame count and storage (rcabf_autotune):
+        later calls plan with it.  Overwrites the arguments' output."""
+        r = L.TuneResult()
+        r.struct_size = C.sizeof(L.TuneResult)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().rcabf_autotune(C.c_void_p(geom.ptr), C.byref(a), C.c_void_p(_stream_ptr(stream)),
+                                           iters, C.byref(r)), "rcabf_autotune")
+        return {f: getattr(r, f) for f, _ in L.TuneResult._fields_ if f != "struct_size"}
+
     def workspace_bytes(self, geom: GeometryHandle, a: L.BeamformArgs) -> int:
         n = C.c_size_t()
         L.check(L.lib().rcabf_beamform_workspace_size(C.c_void_p(geom.ptr), C.byref(a), C.byref(n)),

@@ -122,7 +122,7 @@ int choose_fb(const rcabf_geometry *g, int store, int64_t n_frame, int requested
     return best;
 }
 
-int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
+int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, const TuneChoice *force)
 {
     if (!g || !a) return RCABF_ERR_INVALID_ARGUMENT;
     if (a->struct_size != (int32_t)sizeof(rcabf_beamform_args)) return RCABF_ERR_INVALID_ARGUMENT;
@@ -142,6 +142,16 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
     }
     p.store = a->storage;
     const int es = store_bytes(p.store);
+    TuneChoice tuned;
+    if (!force) {   // a choice the autotuner measured for this geometry, frames and storage
+        std::lock_guard<std::mutex> lk(g->mu);
+        auto it = g->tuned.find({a->n_frame, (int64_t)a->storage});
+        if (it != g->tuned.end() && (fb_req == 0 || fb_req == it->second.fb) &&
+            !(it->second.vb && a->kernel == RCABF_KERNEL_FUSED_NOBLOCK)) {
+            tuned = it->second;
+            force = &tuned;
+        }
+    }
     auto layout = [&](int tile_v_extent) {
         p.n_fb = (int)((a->n_frame + p.fb - 1) / p.fb);
         p.tiles_z = (int)((g->n_z + p.ts.tz - 1) / p.ts.tz);
@@ -163,19 +173,26 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
 
     // Voxel-blocked kernel: exact tables, a steering axis to block along,
     // frames in pairs, and at most 2 rows of shift inside a block.
-    const bool vb_fb_ok = fb_req == 0 ? a->n_frame >= 2 : (fb_req == 2 || fb_req == 4 || fb_req == 8 || fb_req == 16);
+    const bool vb_fb_ok = force ? force->vb == 1
+                                : fb_req == 0 ? a->n_frame >= 2
+                                              : (fb_req == 2 || fb_req == 4 || fb_req == 8 || fb_req == 16);
     if (g->mode == MODE_EXACT && vb_fb_ok && a->kernel != RCABF_KERNEL_FUSED_NOBLOCK) {
         const int d = g->vb_shift(VB_BLOCK);
         if (d >= 1 && d <= 2) {
             const int tu = std::min(4, pow2_ceil(g->n_u));
             const int tvb = 2;
-            const TileShape vts{tu, tvb, VB_THREADS_HOST / (tu * tvb)};
+            TileShape vts{tu, tvb, VB_THREADS_HOST / (tu * tvb)};
+            if (force) {
+                if (force->ts.tu * force->ts.tv * force->ts.tz != VB_THREADS_HOST) return RCABF_ERR_UNSUPPORTED;
+                vts = force->ts;
+            }
             const int need = (int)std::min<int64_t>(
                 g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
             int fb = 0;
             for (int c : {16, 8, 4, 2}) {
-                if (fb_req > 0 && c != fb_req) continue;
-                if (fb_req == 0 && c > 2 * a->n_frame) continue;
+                if (force && c != force->fb) continue;
+                if (!force && fb_req > 0 && c != fb_req) continue;
+                if (!force && fb_req == 0 && c > 2 * a->n_frame) continue;
                 const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
                                                                        fused_row_words(c) * 4)),
                                               vb_stage_rows_cap(p.store, c));
@@ -193,12 +210,18 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p)
             }
         }
     }
+    if (force && force->vb) return RCABF_ERR_UNSUPPORTED;
 
     p.ts = default_tile(g);
+    if (force && force->ts.tu > 0) {
+        if (force->ts.tu * force->ts.tv * force->ts.tz != FUSED_THREADS) return RCABF_ERR_UNSUPPORTED;
+        p.ts = force->ts;
+    }
     // the largest window of any (tile, tx, rx) step, rounded up: the staging
     // buffers hold it, so the kernel never needs a fallback path
     const int need = std::min<int64_t>(g->window_rows(p.ts), a->n_sample);
-    p.fb = choose_fb(g, p.store, a->n_frame, fb_req, need);
+    p.fb = choose_fb(g, p.store, a->n_frame, force ? force->fb : fb_req, need);
+    if (force && p.fb != force->fb) return RCABF_ERR_UNSUPPORTED;
     if (p.fb == 0) {  // no staging buffer holds the window: one-frame kernel
         p.kernel = RCABF_KERNEL_PLAIN;
         p.total = 0;
@@ -301,11 +324,20 @@ static int check_ptrs(const rcabf_beamform_args *a, const Plan &p)
     return RCABF_OK;
 }
 
+static int beamform_planned(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, cudaStream_t st);
+
 int beamform_one(rcabf_geometry *g, const rcabf_beamform_args *a, cudaStream_t st)
 {
     Plan p;
     int s = plan_beamform(g, a, p);
     if (s != RCABF_OK) return s;
+    return beamform_planned(g, a, p, st);
+}
+
+// One beamform call with a given plan (the autotuner's candidates).
+static int beamform_planned(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, cudaStream_t st)
+{
+    int s;
     if ((s = check_ptrs(a, p)) != RCABF_OK) return s;
     device_state(g->device);
     mark(a, 0, st);
@@ -590,6 +622,125 @@ int rcabf_beamform_batch(int n, const rcabf_geometry *const *gs, const rcabf_bea
         if (me != cudaSuccess) return cuda_fail(me, "mask kernel launch");
         g_launches += 1;
     }
+    return RCABF_OK;
+}
+
+int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void *stream, int iters,
+                   rcabf_tune_result *res)
+{
+    if (!gc) return RCABF_ERR_BAD_HANDLE;
+    if (!a || !res || res->struct_size != (int32_t)sizeof(rcabf_tune_result) || iters < 1 || iters > 100)
+        return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->kernel == RCABF_KERNEL_PLAIN) return RCABF_ERR_UNSUPPORTED;
+    rcabf_geometry *g = const_cast<rcabf_geometry *>(gc);
+    cudaStream_t st = (cudaStream_t)stream;
+    // the candidates overwrite out; nothing accumulates, no mask, no stage events
+    rcabf_beamform_args b = *a;
+    b.accumulate = 0;
+    b.mask = nullptr;
+    b.stage_events = nullptr;
+    b.frames_per_block = 0;
+    b.workspace = nullptr;
+    b.workspace_bytes = 0;
+    const std::array<int64_t, 2> key{a->n_frame, (int64_t)a->storage};
+    {
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->tuned.erase(key);   // measure from the planner's own choice
+    }
+    Plan p0;
+    int s = plan_beamform(g, &b, p0);
+    if (s != RCABF_OK) return s;
+    if (p0.kernel != RCABF_KERNEL_FUSED) return RCABF_ERR_UNSUPPORTED;
+
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return cuda_fail(cudaGetLastError(), "autotune events");
+    int tried = 0;
+    auto time_plan = [&](const Plan &p, double &ms) -> int {
+        if (p.total > ws_bytes) {
+            if (ws) cudaFree(ws);
+            ws = nullptr;
+            ws_bytes = 0;
+            const cudaError_t me = cudaMalloc(&ws, p.total);
+            if (me != cudaSuccess) { cudaGetLastError(); return RCABF_ERR_WORKSPACE_TOO_SMALL; }
+            ws_bytes = p.total;
+        }
+        b.workspace = ws;
+        b.workspace_bytes = ws_bytes;
+        int r = beamform_planned(g, &b, p, st);   // first run: kernel attributes, caches
+        if (r != RCABF_OK) return r;
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < iters && r == RCABF_OK; ++i) r = beamform_planned(g, &b, p, st);
+        cudaEventRecord(e1, st);
+        if (r != RCABF_OK) return r;
+        const cudaError_t se = cudaEventSynchronize(e1);
+        if (se != cudaSuccess) return cuda_fail(se, "autotune");
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms = t / iters;
+        ++tried;
+        return RCABF_OK;
+    };
+
+    double default_ms = 0.0;
+    s = time_plan(p0, default_ms);
+    TuneChoice best{p0.vb, p0.fb, p0.ts};
+    double best_ms = default_ms;
+    auto consider = [&](const TuneChoice &c) {
+        Plan p;
+        if (plan_beamform(g, &b, p, &c) != RCABF_OK) return;   // does not fit
+        double ms = 0.0;
+        if (time_plan(p, ms) != RCABF_OK) { cudaGetLastError(); return; }
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    };
+    if (s == RCABF_OK) {
+        if (p0.vb) {
+            // tile shapes (lanes along u, voxel blocks along v, depth) at the
+            // planner's frame block, then frame blocks at the best tile
+            const TileShape tiles[] = {{4, 2, 16}, {2, 4, 16}, {4, 4, 8}, {8, 2, 8}, {2, 2, 32}, {8, 1, 16},
+                                       {4, 1, 32}, {1, 4, 32}};
+            for (const TileShape &t : tiles) {
+                if (t.tu == p0.ts.tu && t.tv == p0.ts.tv && t.tz == p0.ts.tz) continue;
+                consider(TuneChoice{1, p0.fb, t});
+            }
+            const TileShape bt = best.ts;
+            for (int fb : {2, 4, 8, 16}) {
+                if (fb == p0.fb || fb > 2 * a->n_frame) continue;
+                consider(TuneChoice{1, fb, bt});
+            }
+        }
+        // the one-voxel-per-thread kernel at its own frame blocks
+        rcabf_beamform_args nb = b;
+        nb.kernel = RCABF_KERNEL_FUSED_NOBLOCK;
+        Plan pn;
+        if (plan_beamform(g, &nb, pn) == RCABF_OK && pn.kernel == RCABF_KERNEL_FUSED) {
+            for (int fb : {pn.fb, 40, 16}) {
+                if (!fb_supported(g->mode, fb) || (fb != pn.fb && fb > 2 * a->n_frame)) continue;
+                if (!p0.vb && fb == p0.fb) continue;   // the default itself
+                consider(TuneChoice{0, fb, pn.ts});
+            }
+        }
+    }
+    if (ws) cudaFree(ws);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s != RCABF_OK) return s;
+    {
+        std::lock_guard<std::mutex> lk(g->mu);
+        g->tuned[key] = best;
+    }
+    Plan pb;
+    plan_beamform(g, &b, pb);
+    res->voxel_blocked = pb.vb;
+    res->frames_per_block = pb.fb;
+    res->tile_u = pb.ts.tu;
+    res->tile_v = pb.vb ? pb.ts.tv * VB_BLOCK : pb.ts.tv;
+    res->tile_z = pb.ts.tz;
+    res->window_rows = pb.wmax;
+    res->candidates = tried;
+    res->best_ms = best_ms;
+    res->default_ms = default_ms;
     return RCABF_OK;
 }
 

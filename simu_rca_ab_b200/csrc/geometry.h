@@ -24,6 +24,14 @@ struct TileShape {
     }
 };
 
+// A launch choice the autotuner can force on the planner: kernel family,
+// frame block and tile shape (voxel-blocked: tv counts voxel blocks).
+struct TuneChoice {
+    int vb = 0;
+    int fb = 0;
+    TileShape ts{0, 0, 0};
+};
+
 // Spread of the table delay inside the tiles of one shape, used to size the
 // shared-memory window (see window_rows()).
 struct TileSpread {
@@ -74,6 +82,8 @@ struct rcabf_geometry {
     // row shift bound D of the voxel-blocked kernel; -1 if not applicable.
     int vb_shift(int block);
     std::map<int, int> vb_shifts;
+    // launch choices found by rcabf_autotune, keyed by (frames, storage)
+    std::map<std::array<int64_t, 2>, rcabf::TuneChoice> tuned;
 };
 
 namespace rcabf {

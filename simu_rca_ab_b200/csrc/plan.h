@@ -27,7 +27,10 @@ struct Plan {
     int64_t n_items = 0;
 };
 
-int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p);
+// force: a launch choice to plan instead of the planner's own (autotuner);
+// without one, a choice rcabf_autotune stored for these frames and storage
+// is used.  RCABF_ERR_UNSUPPORTED when a forced choice does not fit.
+int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, const TuneChoice *force = nullptr);
 
 // Frame-block sizes with a compiled fused-kernel variant.
 bool fb_supported(int mode, int fb);

@@ -43,7 +43,8 @@ def test_status_strings_carry_reference_identifiers():
 def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     structs = {"g": (L.GeometryDesc, "rcabf_geometry_desc"), "b": (L.BeamformArgs, "rcabf_beamform_args"),
-               "c": (L.ServerConfig, "rcabf_server_config"), "s": (L.ServerStats, "rcabf_server_stats")}
+               "c": (L.ServerConfig, "rcabf_server_config"), "s": (L.ServerStats, "rcabf_server_stats"),
+               "t": (L.TuneResult, "rcabf_tune_result")}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rcabf.h"', "int main(void){"]
     for tag, (py, cname) in structs.items():
         lines.append(f'printf("{tag} %zu\\n", sizeof({cname}));')

@@ -320,3 +320,45 @@ def test_cuda_graph_capture_replays_the_same_bits(bf, c2_small):
     n = C.c_int64()
     L.check(L.lib().rcabf_take_error_count(C.byref(n)))
     assert n.value == 0
+
+
+def test_autotune_keeps_the_fastest_choice_and_the_result(bf, c2_small):
+    """rcabf_autotune times tile shapes / frame blocks / kernel families on
+    the C2 geometry and later plans use its choice; the tuned result agrees
+    with the planner's own within the cross-kernel tolerance."""
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200.params import normalize
+    w, data = c2_small
+    eng = bf.Engine("cuda")          # a geometry of its own: the tuned choice stays here
+    g0 = w.groups[0]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geom = eng.geometry(normalize(np.zeros(1, np.complex64), g0.Geometry, g0.Transmit, w.Param, w.Options))
+    iq = data.contiguous().to(torch.complex32)
+
+    def call():
+        out = torch.empty((w.n_frame, 1, geom.n_pix), dtype=torch.complex64, device="cuda")
+        a = eng.make_args(geom, iq, iq_dtype=L.IQ_C32, n_sample=w.n_sample, n_frame=w.n_frame, out=out,
+                          mask=None, compound=True, storage=L.STORE_F16)
+        return out, a
+
+    before, a = call()
+    plan0 = eng.plan(geom, a)
+    eng.run(geom, a)
+    torch.cuda.synchronize()
+    scratch, a2 = call()
+    res = eng.autotune(geom, a2, iters=1)
+    assert res["candidates"] >= 2 and res["best_ms"] <= res["default_ms"] + 1e-6
+    after, a3 = call()
+    plan1 = eng.plan(geom, a3)
+    assert plan1["frames_per_block"] == res["frames_per_block"]
+    assert plan1["tile"] == [res["tile_u"], res["tile_v"], res["tile_z"]]
+    assert plan1["kernel"] == ("fused_voxel_blocked" if res["voxel_blocked"] else "fused")
+    eng.run(geom, a3)
+    torch.cuda.synchronize()
+    assert H.rel_rms(after.cpu().numpy(), before.cpu().numpy()) < 1e-4
+    if plan1["kernel"] == plan0["kernel"]:
+        assert torch.equal(after, before)   # tile and frame block change no arithmetic
+    print("autotune", res, "default plan", plan0)
+    eng.close()
