@@ -34,6 +34,14 @@ HERE = Path(__file__).resolve().parent
 LIB_ORACLE = HERE / "_build" / "liboracle.so"
 LIB_REF_CPU = HERE / "_ref" / "librca_ref_cpu.so"
 LIB_REF_GPU = {v: HERE / "_ref" / f"librca_ref_gpu_{v}.so" for v in ("strict", "fast", "default")}
+# reference kernel variants (oracle/ref_variant.h): aberration law per element
+# (ab1) or per (transmit, element) (ab2), one output per receive element
+# (nosum), both (nosumab)
+KERNEL_VARIANTS = ("ab1", "ab2", "nosum", "nosumab")
+LIB_REF_CPU_VAR = {k: HERE / "_ref" / f"librca_ref_cpu_{k}.so" for k in KERNEL_VARIANTS}
+LIB_REF_GPU_VAR = {k: HERE / "_ref" / f"librca_ref_gpu_strict_{k}.so" for k in KERNEL_VARIANTS}
+_HAS_AB = {"base": False, "ab1": True, "ab2": True, "nosum": False, "nosumab": True}
+_PER_CH = {"base": False, "ab1": False, "ab2": False, "nosum": True, "nosumab": True}
 
 INTERP_QUAD3, INTERP_REF6, INTERP_LANCZOS = 0, 1, 2
 
@@ -166,12 +174,22 @@ def _load(path: Path):
     return _libs[path]
 
 
-def have_ref_cpu() -> bool:
-    return LIB_REF_CPU.exists()
+def have_ref_cpu(kernel: str = "base") -> bool:
+    return (LIB_REF_CPU if kernel == "base" else LIB_REF_CPU_VAR[kernel]).exists()
 
 
-def have_ref_gpu(variant="strict") -> bool:
-    return LIB_REF_GPU[variant].exists()
+def have_ref_gpu(variant="strict", kernel: str = "base") -> bool:
+    return (LIB_REF_GPU[variant] if kernel == "base" else LIB_REF_GPU_VAR[kernel]).exists()
+
+
+def _ab_arg(kernel: str, ab_law):
+    """The aberration law as the reference variants take it: float32 seconds,
+    [element] (ab1, nosumab) or [transmit][element] (ab2)."""
+    if not _HAS_AB[kernel]:
+        return None
+    if ab_law is None:
+        raise ValueError(f"kernel variant {kernel} needs an aberration law")
+    return np.ascontiguousarray(ab_law, dtype=np.float32).ravel()
 
 
 def _kernel_args(r: RefArgs, data_ptr, out_ptr, mask_ptr, ptrs=None):
@@ -183,13 +201,17 @@ def _kernel_args(r: RefArgs, data_ptr, out_ptr, mask_ptr, ptrs=None):
             C.c_float(r.c), C.c_float(r.t0), C.c_float(r.fnumber)]
 
 
-def run_ref_cpu(r: RefArgs, threads: int | None = None):
-    """O1: reference kernel source on the host.  Returns per-transmit
-    (dataBf [frame][tx][pix] complex64, mask [tx][pix])."""
-    L = _load(LIB_REF_CPU)
-    out = np.zeros((r.n_frame, r.n_tx, r.n_pix, 2), np.float32)
+def run_ref_cpu(r: RefArgs, threads: int | None = None, kernel: str = "base", ab_law=None):
+    """O1: a reference kernel source on the host.  Returns per-transmit
+    (dataBf [frame][tx][pix] complex64 -- [channel][frame][tx][pix] for the
+    per-channel variants -- and mask [tx][pix])."""
+    L = _load(LIB_REF_CPU if kernel == "base" else LIB_REF_CPU_VAR[kernel])
+    shape = ((r.n_ch,) if _PER_CH[kernel] else ()) + (r.n_frame, r.n_tx, r.n_pix, 2)
+    out = np.zeros(shape, np.float32)
     mask = np.zeros((r.n_tx, r.n_pix), np.float32)
+    ab = _ab_arg(kernel, ab_law)
     args = _kernel_args(r, _p(r.data), _p(out), _p(mask))
+    args.insert(-1, _p(ab) if ab is not None else None)   # AbLawRx comes before fnumber
     args += [C.c_int(r.n_pix), C.c_int(r.n_ch), C.c_int(r.n_tx), C.c_int(r.n_frame), C.c_int(r.n_sample),
              C.c_int(int(r.lanczos)), C.c_int(int(r.mask_transmit)), C.c_int(threads or n_threads())]
     L.rca_ref_cpu_run.restype = C.c_int
@@ -264,11 +286,16 @@ def active_units(r: RefArgs, interp: int, lanczos_a: int = 0, threads: int | Non
         C.c_int(lo), C.c_int(hi), C.c_int(threads or n_threads())))
 
 
-def run_ref_gpu(r: RefArgs, variant: str = "strict"):
-    """O2: reference kernel source on the GPU (torch for device memory).
-    Frames are chunked as the reference wrapper does (RCA.m:587-594)."""
+def run_ref_gpu(r: RefArgs, variant: str = "strict", kernel: str = "base", ab_law=None):
+    """O2: a reference kernel source on the GPU (torch for device memory).
+    Frames are chunked as the reference wrapper does (RCA.m:587-594).
+    Per-channel variants return [channel][frame][tx][pix]."""
     import torch
-    L = _load(LIB_REF_GPU[variant])
+    if kernel != "base" and variant != "strict":
+        raise ValueError("the kernel variants are built strict only")
+    L = _load(LIB_REF_GPU[variant] if kernel == "base" else LIB_REF_GPU_VAR[kernel])
+    per_ch = _PER_CH[kernel]
+    ab = _ab_arg(kernel, ab_law)
     L.rca_ref_gpu_launch.restype = C.c_int
     dev = torch.device("cuda")
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -277,23 +304,29 @@ def run_ref_gpu(r: RefArgs, variant: str = "strict"):
     max_siz = 2 ** 31 - 1
     n_chunks = int(np.ceil(2 * r.n_pix * r.n_tx * r.n_frame / max_siz))
     bounds = np.round(np.linspace(0, r.n_frame, n_chunks + 1)).astype(int)
-    out = np.zeros((r.n_frame, r.n_tx, r.n_pix), np.complex64)
+    out = np.zeros(((r.n_ch,) if per_ch else ()) + (r.n_frame, r.n_tx, r.n_pix), np.complex64)
     mask = None
     mask_d = torch.zeros((r.n_tx, r.n_pix), dtype=torch.float32, device=dev)
+    ab_d = t(ab) if ab is not None else None
     st = torch.cuda.current_stream().cuda_stream
     for k in range(n_chunks):
         f0, f1 = bounds[k], bounds[k + 1]
         dchunk = t(r.data[f0:f1])
-        ob = torch.zeros((f1 - f0, r.n_tx, r.n_pix, 2), dtype=torch.float32, device=dev)
+        ob = torch.zeros(((r.n_ch,) if per_ch else ()) + (f1 - f0, r.n_tx, r.n_pix, 2), dtype=torch.float32,
+                         device=dev)
         args = _kernel_args(r, C.cast(C.c_void_p(dchunk.data_ptr()), _f), C.cast(C.c_void_p(ob.data_ptr()), _f),
                             C.cast(C.c_void_p(mask_d.data_ptr()), _f), dptr)
+        args.insert(-1, C.cast(C.c_void_p(ab_d.data_ptr()), _f) if ab_d is not None else None)
         args += [C.c_int(r.n_pix), C.c_int(r.n_ch), C.c_int(r.n_tx), C.c_int(int(f1 - f0)), C.c_int(r.n_sample),
                  C.c_int(int(r.lanczos)), C.c_int(int(r.mask_transmit)), C.c_void_p(st)]
         rc = L.rca_ref_gpu_launch(*args)
         assert rc == 0, rc
         torch.cuda.synchronize()
         o = ob.cpu().numpy()
-        out[f0:f1] = o[..., 0] + 1j * o[..., 1]
+        if per_ch:
+            out[:, f0:f1] = o[..., 0] + 1j * o[..., 1]
+        else:
+            out[f0:f1] = o[..., 0] + 1j * o[..., 1]
         if mask is None:
             mask = mask_d.cpu().numpy().copy()
     return out, mask

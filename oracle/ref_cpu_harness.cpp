@@ -1,9 +1,10 @@
 /*
  * oracle/ref_cpu_harness.cpp -- TEST INFRASTRUCTURE ONLY (oracle "O1").
  *
- * Runs the reference RCA kernel, compiled from its own unmodified source
- * (MATLAB/lib/beamformer/RCA/bfVirtualSourceGeneric_RCA.cu, included below
- * through the include path set by oracle/Makefile), on the host cores.  The
+ * Runs a reference RCA kernel, compiled from its own unmodified source
+ * (MATLAB/lib/beamformer/RCA/bfVirtualSourceGeneric_RCA.cu, or one of its
+ * aberration-law / per-channel variants: ref_variant.h, selected by
+ * oracle/Makefile), on the host cores.  The
  * launch geometry is the one the reference wrapper uses
  * (bfVirtualSourceGeneric_RCA.m:645-650): blocks of 1024 threads, grid
  * [ceil(nPix/1024), nTx, nFrame].  OpenMP spreads the blocks over threads;
@@ -15,7 +16,7 @@
  * any order.
  */
 #include "ref_shim.h"
-#include "bfVirtualSourceGeneric_RCA.cu"
+#include "ref_variant.h"
 
 #include <omp.h>
 
@@ -27,11 +28,13 @@ extern "C" int rca_ref_cpu_run(
     const float *minDist, int flagReceiveX,
     float apertureX, float apertureY, float apertureZ,
     float samplingFrequency, float demodulationFrequency, float speedOfSound,
-    float startTime, float fnumber,
+    float startTime, const float *abLaw, float fnumber,
     int nPix, int nChannel, int nTx, int nFrame, int nSample,
     int flagLanczos, int flagMaskTransmit, int nThreads)
 {
     if (nPix <= 0 || nChannel <= 0 || nTx <= 0 || nFrame <= 0 || nSample <= 0) return 1;
+    if (RCA_HAS_AB && !abLaw) return 3;
+    (void)abLaw;
     const int blk = 1024;
     const int gx = (nPix + blk - 1) / blk;
     const long nBlocks = (long)gx * nTx * nFrame;
@@ -45,12 +48,12 @@ extern "C" int rca_ref_cpu_run(
         blockDim = rm_dim3{(unsigned)blk, 1u, 1u};
         for (unsigned t = 0; t < (unsigned)blk; ++t) {
             threadIdx = rm_dim3{t, 0u, 0u};
-            bfVirtualSourceGeneric_RCA(
+            RCA_KERNEL(
                 dataBf, mask, data, gridBfX, gridBfY, gridBfZ,
                 posEleX, posEleY, posEleZ, vsX, vsY, vsZ, minDist,
                 flagReceiveX != 0, apertureX, apertureY, apertureZ,
                 samplingFrequency, demodulationFrequency, speedOfSound,
-                startTime, fnumber, nPix, nChannel, nTx, nFrame, nSample,
+                startTime, RCA_AB_ARG fnumber, nPix, nChannel, nTx, nFrame, nSample,
                 flagLanczos != 0, flagMaskTransmit != 0);
         }
     }

@@ -13,7 +13,7 @@
  * 32-bit indices stay in range, as the wrapper does (.m:587-594).
  */
 #include <cuda_runtime.h>
-#include "bfVirtualSourceGeneric_RCA.cu"
+#include "ref_variant.h"
 
 extern "C" int rca_ref_gpu_launch(
     float *dataBf, float *mask, const float *data,
@@ -23,7 +23,7 @@ extern "C" int rca_ref_gpu_launch(
     const float *minDist, int flagReceiveX,
     float apertureX, float apertureY, float apertureZ,
     float samplingFrequency, float demodulationFrequency, float speedOfSound,
-    float startTime, float fnumber,
+    float startTime, const float *abLaw, float fnumber,
     int nPix, int nChannel, int nTx, int nFrame, int nSample,
     int flagLanczos, int flagMaskTransmit, void *stream)
 {
@@ -31,12 +31,14 @@ extern "C" int rca_ref_gpu_launch(
     if (nTx > 65535 || nFrame > 65535) return 2;
     dim3 block(1024, 1, 1);
     dim3 grid((nPix + 1023) / 1024, nTx, nFrame);
-    bfVirtualSourceGeneric_RCA<<<grid, block, 0, (cudaStream_t)stream>>>(
+    if (RCA_HAS_AB && !abLaw) return 3;
+    (void)abLaw;
+    RCA_KERNEL<<<grid, block, 0, (cudaStream_t)stream>>>(
         dataBf, mask, data, gridBfX, gridBfY, gridBfZ,
         posEleX, posEleY, posEleZ, vsX, vsY, vsZ, minDist,
         flagReceiveX != 0, apertureX, apertureY, apertureZ,
         samplingFrequency, demodulationFrequency, speedOfSound,
-        startTime, fnumber, nPix, nChannel, nTx, nFrame, nSample,
+        startTime, RCA_AB_ARG fnumber, nPix, nChannel, nTx, nFrame, nSample,
         flagLanczos != 0, flagMaskTransmit != 0);
     return (int)cudaGetLastError();
 }

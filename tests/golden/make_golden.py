@@ -73,9 +73,43 @@ CASES = {
 }
 
 
+# the reference's aberration-law and per-channel kernels (oracle/ref_variant.h):
+# name -> (kernel variant, case arguments, aberration law: None / "ele" / "tx_ele")
+VARIANT_CASES = {
+    "ab1_ref6_rx_x": ("ab1", dict(seed=11, receive_x=True, lanczos=True, mask_tx=False), "ele"),
+    "ab2_quad3_rx_y": ("ab2", dict(seed=12, receive_x=False, lanczos=False, mask_tx=False), "tx_ele"),
+    "nosum_quad3_rx_x_mask": ("nosum", dict(seed=13, receive_x=True, lanczos=False, mask_tx=True,
+                                            grid=(12, 6, 5)), None),
+    "nosumab_ref6_rx_y": ("nosumab", dict(seed=14, receive_x=False, lanczos=True, mask_tx=False,
+                                          grid=(12, 6, 5)), "ele"),
+}
+
+
+def variant_law(kind, n_tx, n_ch, seed):
+    """Seeded receive aberration law (seconds): per element or per (tx, element)."""
+    if kind is None:
+        return None
+    rng = np.random.default_rng(seed + 1000)
+    return rng.uniform(-40e-9, 40e-9, (n_tx, n_ch) if kind == "tx_ele" else n_ch)
+
+
 def main():
     if not H.have_ref_cpu():
         raise SystemExit("oracle/_ref/librca_ref_cpu.so missing: run `make -C oracle` with the reference present")
+    for name, (kernel, kw, ab_kind) in VARIANT_CASES.items():
+        data, G, T, P, O = case(**kw)
+        r = H.prepare(data, G, T, P, O)
+        ab = variant_law(ab_kind, r.n_tx, r.n_ch, kw["seed"])
+        out, mask_tx = H.run_ref_cpu(r, kernel=kernel, ab_law=ab)
+        extra = {} if ab is None else {"ab_law": ab}
+        np.savez_compressed(
+            OUT / f"{name}.npz", data=data, kernel=np.asarray(kernel),
+            **{f"G_{k}": np.asarray(v) for k, v in G.items()},
+            **{f"T_{k}": np.asarray(v) for k, v in T.items()},
+            **{f"P_{k}": np.asarray(v) for k, v in P.items()},
+            **{f"O_{k}": np.asarray(v) for k, v in O.items()},
+            out=out.astype(np.complex64), mask_tx=mask_tx.astype(np.float32), **extra)
+        print(name, out.shape, float(np.abs(out).max()))
     for name, kw in CASES.items():
         data, G, T, P, O = case(**kw)
         r = H.prepare(data, G, T, P, O)
@@ -105,7 +139,7 @@ def load(name: str):
                 d[k[len(prefix):]] = bool(v) if v.dtype == bool else (v.item() if v.ndim == 0 else v)
         return d
 
-    outs = {k: z[k] for k in ("per_tx", "mask_tx", "dataBf", "mask")}
+    outs = {k: z[k] for k in ("per_tx", "mask_tx", "dataBf", "mask", "out", "ab_law", "kernel") if k in z.files}
     return z["data"], grab("G_"), grab("T_"), grab("P_"), grab("O_"), outs
 
 

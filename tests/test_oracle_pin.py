@@ -13,7 +13,7 @@ import pytest
 
 from oracle import fp64 as F64
 from oracle import host as H
-from tests.golden.make_golden import CASES, case, load
+from tests.golden.make_golden import CASES, VARIANT_CASES, case, load
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -76,3 +76,44 @@ def test_reference_fp32_transmit_delay_error_is_visible():
     f1, _ = H.run_fp64(r, H.INTERP_QUAD3)
     rms, _ = H.error_db(c1, f1)
     assert -45 < rms < -20, rms
+
+
+REF_VARIANTS = [("ab1", False, False), ("ab2", False, True), ("nosum", True, None), ("nosumab", True, False)]
+
+
+@pytest.mark.parametrize("kernel,per_channel,ab_per_tx", REF_VARIANTS)
+@pytest.mark.parametrize("rx,lan,mask", [(True, True, False), (False, False, True)])
+def test_c_restatement_matches_reference_variants(kernel, per_channel, ab_per_tx, rx, lan, mask):
+    """The aberration-law kernels (Hyp1_save/..._ab_1.cu, Hyp2/..._ab_2.cu)
+    and the per-channel kernels (NoSum/..._Nosum.cu, NoSum_ab/..._Nosum_ab.cu),
+    compiled from their own sources, against the C restatement with the
+    corresponding option: identical bits."""
+    if not H.have_ref_cpu(kernel):
+        pytest.skip("oracle/_ref variant build missing")
+    data, G, T, P, O = case(61, rx, lan, mask, ns=128)
+    r = H.prepare(data, G, T, P, O)
+    rng = np.random.default_rng(62)
+    ab = None
+    if ab_per_tx is not None:
+        ab = rng.uniform(-40e-9, 40e-9, (r.n_tx, r.n_ch) if ab_per_tx else r.n_ch)
+    o1, m1 = H.run_ref_cpu(r, kernel=kernel, ab_law=ab)
+    c1, cm = H.run_c32(r, per_channel=per_channel, ab_law=ab, ab_per_tx=bool(ab_per_tx))
+    assert o1.shape == c1.shape
+    assert np.array_equal(o1.astype(np.complex64).view(np.float32), c1.astype(np.complex64).view(np.float32))
+    assert np.array_equal(m1, cm)
+    assert np.abs(o1).max() > 0
+
+
+@pytest.mark.parametrize("name", sorted(VARIANT_CASES))
+def test_c_restatement_matches_variant_golden_bitwise(name):
+    """Committed outputs of the reference's aberration-law / per-channel
+    kernels (made by O1, tests/golden/make_golden.py) against the C
+    restatement: identical bits, no reference tree needed."""
+    data, G, T, P, O, outs = load(name)
+    kernel = str(outs["kernel"])
+    r = H.prepare(data, G, T, P, O)
+    ab = outs.get("ab_law")
+    c1, cm = H.run_c32(r, per_channel=kernel.startswith("nosum"), ab_law=ab,
+                       ab_per_tx=ab is not None and np.ndim(ab) == 2)
+    assert np.array_equal(c1.astype(np.complex64).view(np.float32), outs["out"].view(np.float32))
+    assert np.array_equal(cm, outs["mask_tx"])
