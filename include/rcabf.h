@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define RCABF_ABI_VERSION 1
+#define RCABF_ABI_VERSION 2
 
 /* ------------------------------------------------------------------------ */
 /* Status codes                                                              */
@@ -199,7 +199,8 @@ typedef struct rcabf_beamform_args {
     int64_t n_ch, n_tx, n_frame;
     int32_t storage;              /* rcabf_storage */
     int32_t compound;             /* Options.flagCompounding: 1 sum over transmits */
-    void *out;                    /* device complex64: [frame][compound ? 1 : n_tx][pixel] */
+    void *out;                    /* device complex64: [frame][compound ? 1 : n_tx][pixel]
+                                     ([element][frame][tx][pixel] with per_channel) */
     float *mask;                  /* device float: [compound ? 1 : n_tx][pixel]; may be NULL */
     int32_t accumulate;           /* 1: add into out and mask instead of overwriting */
     int32_t kernel;               /* rcabf_kernel */
@@ -211,6 +212,12 @@ typedef struct rcabf_beamform_args {
        after the ingest, after the window-range tables, after the main kernel
        and after the mask kernel (per-stage device timing) */
     void *const *stage_events;
+    /* 1: one output per receive element instead of their sum, out laid out
+       [element][frame][tx][pixel] (the reference's no-sum kernel,
+       NoSum/bfVirtualSourceGeneric_RCA_Nosum.cu:228-229, 275-278, 376-383);
+       needs compound = 0; runs the one-frame kernel */
+    int32_t per_channel;
+    int32_t reserved1;
 } rcabf_beamform_args;
 
 /* Scratch bytes rcabf_beamform needs for these arguments. */

@@ -8,12 +8,12 @@ binding.
 """
 from .params import RCAError, RCAWarning, normalize  # noqa: F401
 
-__all__ = ["bf_rca", "BfIQRCA", "Engine", "RCAError", "RCAWarning", "normalize"]
+__all__ = ["bf_rca", "bf_rca_nosum", "BfIQRCA", "Engine", "RCAError", "RCAWarning", "normalize"]
 
 
 def __getattr__(name):
     # the CUDA-backed names load librcabf on first use
-    if name in ("bf_rca", "BfIQRCA", "Engine", "default_engine", "GeometryHandle"):
+    if name in ("bf_rca", "bf_rca_nosum", "BfIQRCA", "Engine", "default_engine", "GeometryHandle"):
         from . import beamformer
         return getattr(beamformer, name)
     raise AttributeError(name)

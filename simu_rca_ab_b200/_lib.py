@@ -62,6 +62,7 @@ class BeamformArgs(C.Structure):
         ("workspace", C.c_void_p), ("workspace_bytes", C.c_size_t),
         ("frames_per_block", C.c_int32), ("reserved0", C.c_int32),
         ("stage_events", C.POINTER(C.c_void_p)),
+        ("per_channel", C.c_int32), ("reserved1", C.c_int32),
     ]
 
 

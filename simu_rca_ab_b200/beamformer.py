@@ -176,7 +176,7 @@ class Engine:
     def make_args(self, geom: GeometryHandle, iq: "torch.Tensor", *, iq_dtype: int, n_sample: int,
                   n_frame: int, out: "torch.Tensor", mask: "torch.Tensor | None", compound: bool,
                   storage: int = L.STORE_F32, kernel: int = L.KERNEL_AUTO, accumulate: bool = False,
-                  frames_per_block: int = 0) -> L.BeamformArgs:
+                  frames_per_block: int = 0, per_channel: bool = False) -> L.BeamformArgs:
         # The C ABI takes raw pointers: check every buffer holds what the
         # sizes claim before handing it over.
         T = 1 if compound else geom.n_tx
@@ -187,8 +187,11 @@ class Engine:
         if n_frame < 1 or n_sample < 1 or iq.numel() < need_in or not iq.is_contiguous():
             raise ValueError(f"channel data holds {iq.numel()} elements, {need_in} needed "
                              f"({n_frame} frames x {geom.n_tx} tx x {geom.n_ele} elements x {n_sample} samples)")
-        if out.dtype != torch.complex64 or out.numel() < n_frame * T * geom.n_pix or not out.is_contiguous():
-            raise ValueError("out must be a contiguous complex64 tensor of frames x (1 or tx) x pixels")
+        if per_channel and compound:
+            raise ValueError("per-channel output has no compounding over transmits")
+        n_out = n_frame * T * geom.n_pix * (geom.n_ele if per_channel else 1)
+        if out.dtype != torch.complex64 or out.numel() < n_out or not out.is_contiguous():
+            raise ValueError("out must be a contiguous complex64 tensor of ([element] x) frames x (1 or tx) x pixels")
         if mask is not None and (mask.dtype != torch.float32 or mask.numel() < T * geom.n_pix):
             raise ValueError("mask must be a float32 tensor of (1 or tx) x pixels")
         for t in (iq, out) + ((mask,) if mask is not None else ()):
@@ -206,6 +209,7 @@ class Engine:
         a.accumulate = 1 if accumulate else 0
         a.kernel = kernel
         a.frames_per_block = frames_per_block
+        a.per_channel = 1 if per_channel else 0
         return a
 
     def plan(self, geom: GeometryHandle, a: L.BeamformArgs) -> dict:
@@ -377,6 +381,41 @@ def bf_rca(data, Geometry, Transmit, Param, Options=None, *, engine: Engine | No
     s1, s2, s3 = acq.grid.shape
     # [frame][tx][pixel], pixel column-major over the grid -> MATLAB order
     dataBf = out.view(n_frame, T, s3, s2, s1).permute(4, 3, 2, 1, 0)
+    maskv = mask.view(T, s3, s2, s1).permute(3, 2, 1, 0)
+    as_torch = isinstance(data, torch.Tensor) if return_torch is None else return_torch
+    if as_torch:
+        return dataBf, maskv
+    return dataBf.cpu().numpy(), maskv.cpu().numpy()
+
+
+def bf_rca_nosum(data, Geometry, Transmit, Param, Options=None, *, engine: Engine | None = None,
+                 stream=None, return_torch: bool | None = None):
+    """Drop-in for ``bfVirtualSourceGeneric_RCA_Nosum`` and, with
+    ``Param.AbLawRx`` per element, ``bfVirtualSourceGeneric_RCA_Nosum_ab``
+    (MATLAB/lib/beamformer/NoSum*/…_Nosum*.m): one beamformed value per
+    receive element, no compounding.
+
+    Returns ``(dataBf, mask)``: dataBf [*size(gridBfX), nTx, nFrame, nChannel]
+    complex64 (Nosum.m:716-718) and mask [*size(gridBfX), nTx] float32.
+    """
+    acq = normalize(data, Geometry, Transmit, Param, Options)
+    eng = engine or default_engine()
+    geom = eng.geometry(acq, stream=stream)
+    t, iq_dtype, n_sample, n_ch, n_event = _prepare_data(data, acq, eng.device)
+    if n_ch != geom.n_ele:
+        raise RCAError("posEleInvalid", f"data has {n_ch} channels but {geom.n_ele} element positions")
+    if n_event % geom.n_tx:
+        raise RCAError("virtualSourcesNotSameLength",
+                       f"{n_event} events are not a whole number of frames of {geom.n_tx} transmits")
+    n_frame = n_event // geom.n_tx
+    T = geom.n_tx
+    out = torch.empty((geom.n_ele, n_frame, T, geom.n_pix), dtype=torch.complex64, device=eng.device)
+    mask = torch.empty((T, geom.n_pix), dtype=torch.float32, device=eng.device)
+    a = eng.make_args(geom, t, iq_dtype=iq_dtype, n_sample=n_sample, n_frame=n_frame, out=out, mask=mask,
+                      compound=False, storage=acq.storage, kernel=L.KERNEL_PLAIN, per_channel=True)
+    eng.run(geom, a, stream=stream)
+    s1, s2, s3 = acq.grid.shape
+    dataBf = out.view(geom.n_ele, n_frame, T, s3, s2, s1).permute(5, 4, 3, 2, 1, 0)
     maskv = mask.view(T, s3, s2, s1).permute(3, 2, 1, 0)
     as_torch = isinstance(data, torch.Tensor) if return_torch is None else return_torch
     if as_torch:

@@ -134,8 +134,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     if (g->mode == MODE_REF && a->storage != RCABF_STORE_F32) return RCABF_ERR_UNSUPPORTED;
     const int fb_req = a->frames_per_block;
     if (fb_req != 0 && !fb_supported(g->mode, fb_req)) return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->per_channel && a->compound) return RCABF_ERR_INVALID_ARGUMENT;   // no sum over elements: none over tx
     p = Plan{};
-    p.kernel = (a->kernel == RCABF_KERNEL_PLAIN) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
+    p.kernel = (a->kernel == RCABF_KERNEL_PLAIN || a->per_channel) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
     if (p.kernel == RCABF_KERNEL_PLAIN) {
         p.total = 0;
         return RCABF_OK;
@@ -347,6 +348,7 @@ static int beamform_planned(rcabf_geometry *g, const rcabf_beamform_args *a, con
         PlainParams pp{};
         pp.g = g->dev(); pp.iq = a->iq; pp.iq_dtype = a->iq_dtype; pp.n_sample = (int)a->n_sample;
         pp.n_frame = a->n_frame; pp.compound = a->compound ? 1 : 0; pp.accumulate = a->accumulate ? 1 : 0;
+        pp.per_channel = a->per_channel ? 1 : 0;
         pp.out = reinterpret_cast<float2 *>(a->out);
         pp.err_count = device_state(g->device)->err;
         for (int64_t f = 0; f < a->n_frame; ++f) {

@@ -46,7 +46,10 @@ template <int MODE, int KIND, int IQ>
 static cudaError_t plain_do(const PlainParams &p, cudaStream_t st)
 {
     const int64_t n = p.g.n_z * p.g.n_u * p.g.n_v;
-    plain_das_kernel<MODE, KIND, IQ><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);
+    if (p.per_channel)
+        plain_das_kernel<MODE, KIND, IQ, true><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);
+    else
+        plain_das_kernel<MODE, KIND, IQ, false><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);
     return cudaGetLastError();
 }
 

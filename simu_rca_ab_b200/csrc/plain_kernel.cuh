@@ -22,7 +22,10 @@ __device__ __forceinline__ float2 load_iq(const void *base, int64_t i)
     }
 }
 
-template <int MODE, int KIND, int IQ>
+// PC: one output per receive element instead of the sum over them (the
+// reference's no-sum kernel, NoSum/..._Nosum.cu:228-229, 275-278, 376-383):
+// out[element][frame][tx][pix] = the element's term, 0 where it has none.
+template <int MODE, int KIND, int IQ, bool PC>
 __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ PlainParams prm)
 {
     using KT = KindTraits<KIND>;
@@ -42,6 +45,14 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
         const float4 t = __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey]);
         bool cone_ok = ((MODE == MODE_EXACT) ? t.w : t.y) != 0.0f;
         if (g.cone_u != nullptr) cone_ok = cone_ok && g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
+        if constexpr (PC) {
+            if (!cone_ok) {   // masked: every element's term is 0
+                for (int rx = 0; rx < g.n_ele; ++rx) {
+                    float2 *o = prm.out + (((int64_t)rx * prm.n_frame + prm.frame) * g.n_tx + tx) * g.n_pix + pix;
+                    if (!prm.accumulate) *o = make_float2(0.f, 0.f);
+                }
+            }
+        }
         if (cone_ok) {
             const int64_t chan0 = (prm.frame * g.n_tx + tx) * (int64_t)g.n_ele;
             for (int rx = 0; rx < g.n_ele; ++rx) {
@@ -52,7 +63,13 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
                     setup_exact<KIND>(t, e, ab, ab_phasor(g, tx, rx), prm.n_sample, st);
                 else
                     setup_ref<KIND>(t, e, ab, g.ref, prm.n_sample, st);
-                if (!st.ok) continue;
+                if (!st.ok) {
+                    if constexpr (PC) {
+                        float2 *o = prm.out + (((int64_t)rx * prm.n_frame + prm.frame) * g.n_tx + tx) * g.n_pix + pix;
+                        if (!prm.accumulate) *o = make_float2(0.f, 0.f);
+                    }
+                    continue;
+                }
                 const int64_t base = (chan0 + rx) * prm.n_sample + st.n0 - KT::LO;
                 float2 tsum = make_float2(0.f, 0.f);
 #pragma unroll
@@ -68,6 +85,21 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
                         tsum.y = __fadd_rn(tsum.y, __fmul_rn(st.w[j], x.y));
                     }
                 }
+                if constexpr (PC) {   // the element's own term, written as the reference's no-sum kernel does
+                    float2 term;
+                    if constexpr (MODE == MODE_EXACT) {
+                        term.x = fmaf(st.P.x, tsum.x, -st.P.y * tsum.y);
+                        term.y = fmaf(st.P.x, tsum.y, st.P.y * tsum.x);
+                    } else {
+                        const float cs = st.P.x, sn = st.P.y;
+                        term.x = __fmul_rn(st.apod, __fadd_rn(__fmul_rn(tsum.x, cs), __fmul_rn(tsum.y, sn)));
+                        term.y = __fmul_rn(st.apod, __fadd_rn(__fmul_rn(-tsum.x, sn), __fmul_rn(tsum.y, cs)));
+                    }
+                    float2 *o = prm.out + (((int64_t)rx * prm.n_frame + prm.frame) * g.n_tx + tx) * g.n_pix + pix;
+                    if (prm.accumulate) { float2 q = *o; q.x += term.x; q.y += term.y; *o = q; }
+                    else *o = term;
+                    continue;
+                }
                 float2 &a = acc_tx[0];
                 if constexpr (MODE == MODE_EXACT) {
                     a.x = fmaf(st.P.x, tsum.x, fmaf(-st.P.y, tsum.y, a.x));
@@ -79,6 +111,10 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
                 }
             }
         }
+        if constexpr (PC) {
+            acc_tx[0] = make_float2(0.f, 0.f);
+            continue;
+        }
         if (!prm.compound) {
             float2 *o = prm.out + (prm.frame * g.n_tx + tx) * g.n_pix + pix;
             if (prm.accumulate) { float2 q = *o; q.x += acc_tx[0].x; q.y += acc_tx[0].y; *o = q; }
@@ -89,7 +125,7 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
         }
         acc_tx[0] = make_float2(0.f, 0.f);
     }
-    if (prm.compound) {
+    if (!PC && prm.compound) {
         float2 *o = prm.out + prm.frame * g.n_pix + pix;
         if (prm.accumulate) { float2 q = *o; q.x += acc[0].x; q.y += acc[0].y; *o = q; }
         else *o = acc[0];

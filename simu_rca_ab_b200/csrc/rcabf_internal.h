@@ -115,6 +115,7 @@ struct PlainParams {
     int64_t frame;
     int64_t n_frame;
     int32_t compound, accumulate;
+    int32_t per_channel;        // out is [element][frame][tx][pix]: one value per receive element
     float2 *out;
     unsigned long long *err_count;
 };

@@ -21,7 +21,7 @@ def header_functions():
 
 def test_library_built_and_loads():
     assert LIB.exists(), "run `python -m simu_rca_ab_b200.build`"
-    assert L.lib().rcabf_abi_version() == 1
+    assert L.lib().rcabf_abi_version() == 2
 
 
 def test_every_declared_symbol_is_exported_and_bound():
