@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the c3 serving-mix measurement")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the step")
     ap.add_argument("--no-autotune", action="store_true", help="use the planner's launch choice untimed")
+    ap.add_argument("--no-clutter", action="store_true", help="skip the SVD clutter filter of the ensemble")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
@@ -445,6 +446,29 @@ def main():
         except Exception as ex:   # reported in the line, the eager number stands
             graph = {"error": f"{type(ex).__name__}: {ex}"}
 
+    # the downstream SVD clutter filter on this ensemble (Gram in FP64,
+    # eigen-decomposition, projection), timed on the device
+    clutter = None
+    if not a.no_clutter and rank == 0:
+        try:
+            from simu_rca_ab_b200.clutter import svd_clutter_filter
+            x = out[:, 0]
+            svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C")
+            torch.cuda.synchronize()
+            c0e, c1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0e.record()
+            xf, ev = svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C")
+            c1e.record()
+            torch.cuda.synchronize()
+            clutter = {"what": "SVDClutterFilter high-pass w=0.1 on the beamformed ensemble "
+                               f"({x.shape[1]} voxels x {x.shape[0]} frames): FP64 Gram (cuBLAS ZGEMM), "
+                               "FP64 eigh, FP32 projection (CGEMM)",
+                       "ms": c0e.elapsed_time(c1e),
+                       "energy_kept": float((xf.abs() ** 2).sum() / (x.abs() ** 2).sum())}
+            del xf
+        except Exception as ex:
+            clutter = {"error": f"{type(ex).__name__}: {ex}"}
+
     # fused-kernel time per launch: stage events of a separate, synchronised step
     step()
     torch.cuda.synchronize()
@@ -575,7 +599,7 @@ def main():
                        "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
-            "serving": serving, "graph": graph,
+            "serving": serving, "graph": graph, "clutter_filter": clutter,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
