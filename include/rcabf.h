@@ -338,6 +338,25 @@ int rcabf_server_get_stats(rcabf_server *s, rcabf_server_stats *st);
 /* Runs the queued requests to completion, then frees the arena and streams. */
 int rcabf_server_destroy(rcabf_server *s);
 
+/* ------------------------------------------------------------------------ */
+/* Simulator (the producer of channel data)                                  */
+/* ------------------------------------------------------------------------ */
+/* Element field of the frequency-domain simulator: for every frequency f,
+ * scatterer s and element e, the sum over the element's sub-elements of
+ * Green's function x azimuth directivity x elevation directivity (flat, or
+ * the 4-Gaussian focused-element model when the elevation focus is within
+ * 10 m) x the lens delay phase.  out: device complex64 [n_f][n_scat][n_ele];
+ * r_scat: device float [3][n_scat] (x, y, z, metres); r_ele: device float
+ * [n_sub][5][n_ele] (x, y, z, azimuth, elevation); kwave: device complex64
+ * [n_f] (wavenumber, imaginary part = attenuation).  Replaces the per-element
+ * body of the reference kernels TXfield / RXfield
+ * (MATLAB/lib/simulator/SimUS_CUDARCA.cu:209-379), which the Python
+ * simulator (simu_rca_ab_b200.simulator) combines with the transmit delays,
+ * apodisations, pulse and impulse responses. */
+int rcabf_sim_element_field(void *out, const float *r_scat, const float *r_ele, const void *kwave, float width,
+                            float height, float rfocus, int baffle, float lens, float speed_of_sound,
+                            int64_t n_scat, int64_t n_ele, int64_t n_f, int64_t n_sub, void *stream);
+
 /* Count of device-side bound-check trips since the last call (expected 0). */
 int rcabf_take_error_count(int64_t *count);
 

@@ -86,6 +86,14 @@ RM_INLINE float rm_cosf(float x) { return (float)cos((double)x); }
 RM_INLINE float rm_sinf(float x) { return (float)sin((double)x); }
 RM_INLINE float rm_acosf(float x) { return (float)acos((double)x); }
 
+/* exp, asin, atan2, sqrt, fabs of float arguments, evaluated in double
+ * (the simulator kernels, SimUS_CUDARCA.cu). */
+RM_INLINE float rm_expf(float x) { return (float)exp((double)x); }
+RM_INLINE float rm_asinf(float x) { return (float)asin((double)x); }
+RM_INLINE float rm_atan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
+RM_INLINE float rm_sqrtf(float x) { return (float)sqrt((double)x); }
+RM_INLINE float rm_fabsf(float x) { return fabsf(x); }
+
 /* 1 / sqrt(x) in double (the reference passes a double argument). */
 RM_INLINE double rm_rsqrt(double x) { return 1.0 / sqrt(x); }
 

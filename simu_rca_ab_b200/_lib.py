@@ -119,6 +119,9 @@ _SIGS = {
     "rcabf_server_wait_for": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(C.c_int)]),
     "rcabf_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "rcabf_server_destroy": (C.c_int, [C.c_void_p]),
+    "rcabf_sim_element_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                          C.c_float, C.c_int, C.c_float, C.c_float, C.c_int64, C.c_int64,
+                                          C.c_int64, C.c_int64, C.c_void_p]),
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_measure_fp32_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
