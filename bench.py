@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the step")
     ap.add_argument("--no-autotune", action="store_true", help="use the planner's launch choice untimed")
     ap.add_argument("--no-clutter", action="store_true", help="skip the SVD clutter filter of the ensemble")
+    ap.add_argument("--no-simulator", action="store_true", help="skip the simulator timing")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
@@ -261,6 +262,52 @@ def serving_leg(eng, dev, n_requests: int, rate_hz: float, seed: int = 3):
                          "how": "plain_das_kernel per request (device time of 2 frames x frames/2), "
                                 "FIFO queue on the same arrival times"},
     }
+
+
+def simulator_leg(dev, seed: int = 7):
+    """The frequency-domain simulator (sim_us_rca) on a 64+64 RCA set-up:
+    transmit rows / receive columns of 64 strips (8 sub-elements each),
+    16 plane waves, 200 scatterers, 2 frames, 1024 samples at 31.2 MHz."""
+    import numpy as np
+    import torch
+
+    from simu_rca_ab_b200.simulator import sim_plan, sim_us_rca
+    rng = np.random.default_rng(seed)
+    n_ele, n_sub, n_tx, n_scat, n_frame = 64, 8, 16, 200, 2
+    pitch, f0, c = 0.3e-3, 7.8e6, 1540.0
+    pos = (np.arange(n_ele) - (n_ele - 1) / 2) * pitch
+    strip = (np.arange(n_sub) - (n_sub - 1) / 2) * (n_ele * pitch / n_sub)
+    tx = np.zeros((n_ele, 5, n_sub))
+    rx = np.zeros((n_ele, 5, n_sub))
+    for q in range(n_sub):
+        tx[:, 0, q], tx[:, 1, q] = strip[q], pos
+        rx[:, 0, q], rx[:, 1, q] = pos, strip[q]
+    t = np.arange(0, 2 / f0, 1 / 250e6)
+    ir = np.sin(2 * np.pi * f0 * t) * np.hanning(t.size)
+    trans = lambda p: {"frequency": f0, "impulseResponse": ir, "lensCorrection": 0.0, "ElementPos": p,
+                       "ElementHeight": 2e-3, "ElementWidth": 0.27e-3, "ElementElevationFocus": 20e-3, "baffle": 1}
+    n_event = n_tx * n_frame
+    base = np.stack([rng.uniform(-9e-3, 9e-3, n_scat), rng.uniform(-9e-3, 9e-3, n_scat),
+                     rng.uniform(5e-3, 25e-3, n_scat), rng.rayleigh(1.0, n_scat)], 1)
+    scat = np.repeat(base[:, :, None], n_event, 2)
+    th = np.deg2rad(np.linspace(-8, 8, n_tx))
+    TXSI = [{"pulseShape": np.sin(2 * np.pi * f0 * t), "Delay": pos * np.sin(a) / c - (pos * np.sin(a) / c).min(),
+             "Apod": np.ones(n_ele)} for a in th]
+    RXSI = [{"samplingFrequency": 4 * f0, "demodFrequency": f0, "startTime": 0.0, "numelSample": 1024,
+             "sampleMode": "NS200BW", "InputFilter": np.array([1.0]), "Apod": np.ones(n_ele)} for _ in th]
+    case = ({"speedOfSound": c, "attenuation": 0.5, "scattererPos": scat}, trans(tx), trans(rx), TXSI, RXSI)
+    sim_us_rca(*case)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    raw = sim_us_rca(*case)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    p = sim_plan(*case)
+    evals = p["n_freq"] * n_scat * n_ele * n_sub * 2 * n_frame   # element-field terms (transmit + receive arrays)
+    return {"what": f"sim_us_rca: {n_ele}+{n_ele} RCA strips x {n_sub} sub-elements, {n_tx} plane waves, "
+                    f"{n_scat} scatterers, {n_frame} frames, {p['n_freq']} frequencies, Raw {list(raw.shape)}",
+            "ms": 1e3 * el, "element_field_terms_per_s": evals / el,
+            "note": "scatterers static within a frame: one element field per frame, all transmits as one GEMM"}
 
 
 def run_reference(a, rank):
@@ -543,6 +590,13 @@ def main():
             serving = {"error": f"{type(ex).__name__}: {ex}"}
         torch.cuda.synchronize()
 
+    sim = None
+    if not a.no_simulator and rank == 0:
+        try:
+            sim = simulator_leg(dev)
+        except Exception as ex:
+            sim = {"error": f"{type(ex).__name__}: {ex}"}
+
     line = None
     if rank == 0:
         from oracle import host as H
@@ -599,7 +653,7 @@ def main():
                        "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
-            "serving": serving, "graph": graph, "clutter_filter": clutter,
+            "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
