@@ -41,7 +41,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "DAS voxel·rx·tx/s (nominal, summed over frames)"
 UNIT = "voxel·rx·tx/s"
 # plan kernel -> CUDA kernel function
-KERNEL_NAMES = {"fused_voxel_blocked": "fused_vb_kernel", "fused": "fused_das_kernel", "plain": "plain_das_kernel"}
+KERNEL_NAMES = {"fused_voxel_blocked": "fused_vb_kernel", "fused_voxel_blocked_tmem": "fused_vb_kernel",
+                "fused": "fused_das_kernel", "plain": "plain_das_kernel"}
 
 
 def parse():
@@ -53,7 +54,9 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling cases)")
     ap.add_argument("--storage", default=None, help="float32 | float16 | bfloat16 (default: workload's)")
-    ap.add_argument("--kernel", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--kernel", default="fused", choices=["fused", "plain", "tmem", "regs"],
+                    help="fused: the planner's (or autotuner's) choice; tmem / regs: the voxel-blocked kernel "
+                         "with tensor-memory / register accumulators")
     ap.add_argument("--frames-per-block", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -374,7 +377,8 @@ def main():
     w = W.get(a.workload, n_frame=a.frames)
     storage = a.storage or w.storage
     st_code = {"float32": L.STORE_F32, "float16": L.STORE_F16, "bfloat16": L.STORE_BF16}[storage]
-    kern = L.KERNEL_PLAIN if a.kernel == "plain" else L.KERNEL_FUSED
+    kern = {"plain": L.KERNEL_PLAIN, "tmem": L.KERNEL_FUSED_TMEM, "regs": L.KERNEL_FUSED_REGS}.get(a.kernel,
+                                                                                                 L.KERNEL_FUSED)
 
     data = W.channel_data(w, seed=rank, device=dev)                       # [F][T][E][S] complex64
     in_dtype = torch.complex32 if storage == "float16" else torch.complex64

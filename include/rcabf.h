@@ -119,7 +119,12 @@ typedef enum rcabf_kernel {
     RCABF_KERNEL_FUSED = 1, /* persistent voxel-tiled shared-memory gather, all frames in one launch;
                                voxel-blocked along the steering axis when the geometry allows */
     RCABF_KERNEL_PLAIN = 2, /* one launch per frame, one thread per voxel, global gathers */
-    RCABF_KERNEL_FUSED_NOBLOCK = 3 /* the fused kernel with one voxel per thread */
+    RCABF_KERNEL_FUSED_NOBLOCK = 3, /* the fused kernel with one voxel per thread */
+    /* the voxel-blocked fused kernel with a given accumulator store
+       (RCABF_ERR_UNSUPPORTED where the geometry allows no voxel blocking):
+       tensor memory (frame blocks of 8 or 16; sm_100a TMEM) or registers */
+    RCABF_KERNEL_FUSED_TMEM = 4,
+    RCABF_KERNEL_FUSED_REGS = 5
 } rcabf_kernel;
 
 /* ------------------------------------------------------------------------ */
@@ -265,7 +270,8 @@ int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a
 /* What rcabf_autotune chose for a geometry, frame count and storage. */
 typedef struct rcabf_tune_result {
     int32_t struct_size;          /* sizeof(rcabf_tune_result) */
-    int32_t voxel_blocked;        /* 1: the voxel-blocked kernel, 0: one voxel per thread */
+    int32_t voxel_blocked;        /* 0: one voxel per thread; the voxel-blocked kernel with its
+                                     accumulators in 1: registers, 2: tensor memory */
     int32_t frames_per_block;
     int32_t tile_u, tile_v, tile_z;   /* voxels per tile along the receive axis, steering axis, depth */
     int32_t window_rows;          /* sample rows staged per step (the shared-memory window depth) */

@@ -135,6 +135,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     const int fb_req = a->frames_per_block;
     if (fb_req != 0 && !fb_supported(g->mode, fb_req)) return RCABF_ERR_INVALID_ARGUMENT;
     if (a->per_channel && a->compound) return RCABF_ERR_INVALID_ARGUMENT;   // no sum over elements: none over tx
+    if (a->kernel < RCABF_KERNEL_AUTO || a->kernel > RCABF_KERNEL_FUSED_REGS) return RCABF_ERR_INVALID_ARGUMENT;
     p = Plan{};
     p.kernel = (a->kernel == RCABF_KERNEL_PLAIN || a->per_channel) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
     if (p.kernel == RCABF_KERNEL_PLAIN) {
@@ -147,8 +148,10 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     if (!force) {   // a choice the autotuner measured for this geometry, frames and storage
         std::lock_guard<std::mutex> lk(g->mu);
         auto it = g->tuned.find({a->n_frame, (int64_t)a->storage});
+        const int vb_req = a->kernel == RCABF_KERNEL_FUSED_TMEM ? 2 : a->kernel == RCABF_KERNEL_FUSED_REGS ? 1 : -1;
         if (it != g->tuned.end() && (fb_req == 0 || fb_req == it->second.fb) &&
-            !(it->second.vb && a->kernel == RCABF_KERNEL_FUSED_NOBLOCK)) {
+            !(it->second.vb && a->kernel == RCABF_KERNEL_FUSED_NOBLOCK) &&
+            (vb_req < 0 || vb_req == it->second.vb)) {
             tuned = it->second;
             force = &tuned;
         }
@@ -173,8 +176,14 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     };
 
     // Voxel-blocked kernel: exact tables, a steering axis to block along,
-    // frames in pairs, and at most 2 rows of shift inside a block.
-    const bool vb_fb_ok = force ? force->vb == 1
+    // frames in pairs, and at most 2 rows of shift inside a block.  Its
+    // accumulators live in registers (vb = 1) or, for frame blocks of 8 and
+    // 16, in tensor memory (vb = 2).
+    const int want_vb = force ? force->vb
+                        : a->kernel == RCABF_KERNEL_FUSED_TMEM ? 2
+                        : a->kernel == RCABF_KERNEL_FUSED_REGS ? 1
+                                                               : 0;   // 0: the planner's choice
+    const bool vb_fb_ok = force ? force->vb >= 1
                                 : fb_req == 0 ? a->n_frame >= 2
                                               : (fb_req == 2 || fb_req == 4 || fb_req == 8 || fb_req == 16);
     if (g->mode == MODE_EXACT && vb_fb_ok && a->kernel != RCABF_KERNEL_FUSED_NOBLOCK) {
@@ -189,29 +198,38 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
             }
             const int need = (int)std::min<int64_t>(
                 g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
-            int fb = 0;
-            for (int c : {16, 8, 4, 2}) {
-                if (force && c != force->fb) continue;
-                if (!force && fb_req > 0 && c != fb_req) continue;
-                if (!force && fb_req == 0 && c > 2 * a->n_frame) continue;
-                const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
-                                                                       fused_row_words(c) * 4)),
-                                              vb_stage_rows_cap(p.store, c));
-                if (cap >= need) { fb = c; break; }
-            }
+            // rows a stage holds: the window, and with tensor-memory
+            // accumulators at least the taps + shift rows every lane reads
+            auto rows_for = [&](int tm) { return tm ? std::max(need, kind_taps(g->kind) + d) : need; };
+            auto pick_fb = [&](int tm) {   // the largest frame block whose window fits
+                for (int c : {16, 8, 4, 2}) {
+                    if (tm && c < 8) continue;
+                    if (force && c != force->fb) continue;
+                    if (!force && fb_req > 0 && c != fb_req) continue;
+                    if (!force && fb_req == 0 && c > 2 * a->n_frame) continue;
+                    const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
+                                                                           fused_row_words(c) * 4)),
+                                                  vb_stage_rows_cap(p.store, c));
+                    if (cap >= rows_for(tm)) return c;
+                }
+                return 0;
+            };
+            int tm = want_vb == 2 ? 1 : want_vb == 1 ? 0 : VB_TMEM_DEFAULT;
+            int fb = pick_fb(tm);
+            if (!fb && tm && want_vb == 0) fb = pick_fb(tm = 0);   // blocks below 8 frames: registers
             if (fb) {
-                p.vb = 1;
+                p.vb = tm ? 2 : 1;
                 p.d = d;
                 p.fb = fb;
                 p.ts = vts;
                 layout(vts.tv * VB_BLOCK);
-                p.wmax = need;
+                p.wmax = rows_for(tm);
                 p.smem = vb_smem_bytes(p.store, p.wmax, p.row_words);
                 return RCABF_OK;
             }
         }
     }
-    if (force && force->vb) return RCABF_ERR_UNSUPPORTED;
+    if (want_vb) return RCABF_ERR_UNSUPPORTED;
 
     p.ts = default_tile(g);
     if (force && force->ts.tu > 0) {
@@ -277,6 +295,31 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
     return RCABF_OK;
 }
 
+// Resident CTAs per SM of the plan's fused kernel at `smem` bytes of dynamic
+// shared memory (sets the kernel's shared-memory limit on first use).
+static int resident_ctas(const rcabf_geometry *g0, const Plan &p, size_t smem, DeviceState *ds, int &occ)
+{
+    // variant: (mode, or 2 vb + row shift for the voxel-blocked kernels; kind; fb; store)
+    const std::array<int64_t, 4> var{p.vb ? 2 * p.vb + p.d : g0->mode, g0->kind, p.fb, p.store};
+    const std::array<int64_t, 5> key{var[0], var[1], var[2], var[3], (int64_t)smem};
+    std::lock_guard<std::mutex> lk(ds->mu);
+    auto lim = ds->smem_limit.find(var);
+    if (lim == ds->smem_limit.end() || lim->second < smem) {
+        const cudaError_t pe = p.vb ? prepare_fused_vb(g0->kind, p.d, p.vb == 2, p.fb, p.store, smem)
+                                    : prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
+        if (pe != cudaSuccess) return cuda_fail(pe, "fused kernel shared-memory attribute");
+        ds->smem_limit[var] = smem;
+    }
+    auto oc = ds->occ.find(key);
+    if (oc == ds->occ.end()) {
+        const int o = p.vb ? fused_vb_occupancy(g0->kind, p.d, p.vb == 2, p.fb, p.store, smem)
+                           : fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
+        oc = ds->occ.emplace(key, o).first;
+    }
+    occ = std::max(1, oc->second);
+    return RCABF_OK;
+}
+
 int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaStream_t st)
 {
     // a counter set by the caller (rcabf_beamform_noalloc) is kept
@@ -284,30 +327,12 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     if (!prm.err_count) prm.err_count = ds->err;
     const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words)
                              : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
-    // variant: (mode, or 2 + row shift for the voxel-blocked kernel; kind; fb; store)
-    const std::array<int64_t, 4> var{p.vb ? 2 + p.d : g0->mode, g0->kind, p.fb, p.store};
-    const std::array<int64_t, 5> key{var[0], var[1], var[2], var[3], (int64_t)smem};
-    int occ;
-    {
-        std::lock_guard<std::mutex> lk(ds->mu);
-        auto lim = ds->smem_limit.find(var);
-        if (lim == ds->smem_limit.end() || lim->second < smem) {
-            const cudaError_t pe = p.vb ? prepare_fused_vb(g0->kind, p.d, p.fb, p.store, smem)
-                                        : prepare_fused(g0->mode, g0->kind, p.fb, p.store, smem);
-            if (pe != cudaSuccess) return cuda_fail(pe, "fused kernel shared-memory attribute");
-            ds->smem_limit[var] = smem;
-        }
-        auto oc = ds->occ.find(key);
-        if (oc == ds->occ.end()) {
-            const int o = p.vb ? fused_vb_occupancy(g0->kind, p.d, p.fb, p.store, smem)
-                               : fused_occupancy(g0->mode, g0->kind, p.fb, p.store, smem);
-            oc = ds->occ.emplace(key, o).first;
-        }
-        occ = std::max(1, oc->second);
-    }
+    int occ = 0;
+    const int so = resident_ctas(g0, p, smem, ds, occ);
+    if (so != RCABF_OK) return so;
     const int64_t grid = std::min<int64_t>(prm.n_items, (int64_t)ds->n_sm * occ);
     if (grid <= 0) return RCABF_OK;
-    const cudaError_t le = p.vb ? launch_fused_vb(g0->kind, p.d, p.fb, p.store, prm, (int)grid, smem, st)
+    const cudaError_t le = p.vb ? launch_fused_vb(g0->kind, p.d, p.vb == 2, p.fb, p.store, prm, (int)grid, smem, st)
                                 : launch_fused(g0->mode, g0->kind, p.fb, p.store, prm, (int)grid, smem, st);
     if (le != cudaSuccess) return cuda_fail(le, "fused kernel launch");
     g_launches += 1;
@@ -558,13 +583,21 @@ int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, c
     Plan p;
     int s = plan_beamform(const_cast<rcabf_geometry *>(g), a, p);
     if (s != RCABF_OK) return s;
-    const char *kname = p.kernel == RCABF_KERNEL_PLAIN ? "plain" : p.vb ? "fused_voxel_blocked" : "fused";
+    int occ = 0;   // resident CTAs per SM of the fused kernel (0: plain kernel)
+    if (p.kernel == RCABF_KERNEL_FUSED) {
+        s = resident_ctas(g, p, p.smem, device_state(g->device), occ);
+        if (s != RCABF_OK) return s;
+    }
+    const char *kname = p.kernel == RCABF_KERNEL_PLAIN ? "plain"
+                        : p.vb == 2                     ? "fused_voxel_blocked_tmem"
+                        : p.vb                          ? "fused_voxel_blocked"
+                                                        : "fused";
     snprintf(buf, len,
              "{\"kernel\": \"%s\", \"row_shift\": %d, \"frames_per_block\": %d, \"frame_blocks\": %d, "
              "\"tile\": [%d, %d, %d], \"voxels_per_thread\": %d, \"window_rows\": %d, \"smem_bytes\": %zu, "
-             "\"workspace_bytes\": %zu, \"work_items\": %lld, \"storage\": %d}",
+             "\"workspace_bytes\": %zu, \"work_items\": %lld, \"storage\": %d, \"ctas_per_sm\": %d}",
              kname, p.d, p.fb, p.n_fb, p.ts.tu, p.vb ? p.ts.tv * VB_BLOCK : p.ts.tv, p.ts.tz, p.vb ? VB_BLOCK : 1,
-             p.wmax, p.smem, p.total, (long long)p.n_items, p.store);
+             p.wmax, p.smem, p.total, (long long)p.n_items, p.store, occ);
     return RCABF_OK;
 }
 
@@ -704,12 +737,18 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
                                        {4, 1, 32}, {1, 4, 32}};
             for (const TileShape &t : tiles) {
                 if (t.tu == p0.ts.tu && t.tv == p0.ts.tv && t.tz == p0.ts.tz) continue;
-                consider(TuneChoice{1, p0.fb, t});
+                consider(TuneChoice{p0.vb, p0.fb, t});
             }
             const TileShape bt = best.ts;
             for (int fb : {2, 4, 8, 16}) {
                 if (fb == p0.fb || fb > 2 * a->n_frame) continue;
-                consider(TuneChoice{1, fb, bt});
+                consider(TuneChoice{p0.vb, fb, bt});
+            }
+            // the other accumulator store (registers / tensor memory) at the
+            // frame blocks tensor memory takes
+            for (int fb : {8, 16}) {
+                if (fb > 2 * a->n_frame) continue;
+                consider(TuneChoice{p0.vb == 2 ? 1 : 2, fb, bt});
             }
         }
         // the one-voxel-per-thread kernel at its own frame blocks

@@ -19,8 +19,8 @@ cudaError_t fused_entry_ref(int kind, int store, int fb, const FusedParams *p, i
 cudaError_t plain_entry_ref(int kind, const PlainParams &p, cudaStream_t st);
 
 #define DECL_VB(NAME)                                                                                \
-    cudaError_t vb_entry_##NAME(int d, int store, int fb, const FusedParams *p, int grid, size_t smem,\
-                                cudaStream_t st, int what, int *occ);
+    cudaError_t vb_entry_##NAME(int d, int tm, int store, int fb, const FusedParams *p, int grid,    \
+                                size_t smem, cudaStream_t st, int what, int *occ);
 DECL_VB(exact_quad3)
 DECL_VB(exact_ref6)
 DECL_VB(exact_l2)
@@ -28,34 +28,34 @@ DECL_VB(exact_l3)
 DECL_VB(exact_l4)
 #undef DECL_VB
 
-static cudaError_t vb_route(int kind, int d, int fb, int store, const FusedParams *p, int grid, size_t smem,
-                            cudaStream_t st, int what, int *occ)
+static cudaError_t vb_route(int kind, int d, int tm, int fb, int store, const FusedParams *p, int grid,
+                            size_t smem, cudaStream_t st, int what, int *occ)
 {
     switch (kind) {
-    case K_QUAD3: return vb_entry_exact_quad3(d, store, fb, p, grid, smem, st, what, occ);
-    case K_REF6: return vb_entry_exact_ref6(d, store, fb, p, grid, smem, st, what, occ);
-    case K_LANCZOS2: return vb_entry_exact_l2(d, store, fb, p, grid, smem, st, what, occ);
-    case K_LANCZOS3: return vb_entry_exact_l3(d, store, fb, p, grid, smem, st, what, occ);
-    case K_LANCZOS4: return vb_entry_exact_l4(d, store, fb, p, grid, smem, st, what, occ);
+    case K_QUAD3: return vb_entry_exact_quad3(d, tm, store, fb, p, grid, smem, st, what, occ);
+    case K_REF6: return vb_entry_exact_ref6(d, tm, store, fb, p, grid, smem, st, what, occ);
+    case K_LANCZOS2: return vb_entry_exact_l2(d, tm, store, fb, p, grid, smem, st, what, occ);
+    case K_LANCZOS3: return vb_entry_exact_l3(d, tm, store, fb, p, grid, smem, st, what, occ);
+    case K_LANCZOS4: return vb_entry_exact_l4(d, tm, store, fb, p, grid, smem, st, what, occ);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_fused_vb(int kind, int d, int fb, int store, const FusedParams &p, int grid, size_t smem,
-                            cudaStream_t st)
+cudaError_t launch_fused_vb(int kind, int d, int tm, int fb, int store, const FusedParams &p, int grid,
+                            size_t smem, cudaStream_t st)
 {
-    return vb_route(kind, d, fb, store, &p, grid, smem, st, 0, nullptr);
+    return vb_route(kind, d, tm, fb, store, &p, grid, smem, st, 0, nullptr);
 }
 
-cudaError_t prepare_fused_vb(int kind, int d, int fb, int store, size_t smem)
+cudaError_t prepare_fused_vb(int kind, int d, int tm, int fb, int store, size_t smem)
 {
-    return vb_route(kind, d, fb, store, nullptr, 0, smem, nullptr, 1, nullptr);
+    return vb_route(kind, d, tm, fb, store, nullptr, 0, smem, nullptr, 1, nullptr);
 }
 
-int fused_vb_occupancy(int kind, int d, int fb, int store, size_t smem)
+int fused_vb_occupancy(int kind, int d, int tm, int fb, int store, size_t smem)
 {
     int occ = 0;
-    if (vb_route(kind, d, fb, store, nullptr, 0, smem, nullptr, 2, &occ) != cudaSuccess) return 0;
+    if (vb_route(kind, d, tm, fb, store, nullptr, 0, smem, nullptr, 2, &occ) != cudaSuccess) return 0;
     return occ;
 }
 

@@ -4,6 +4,8 @@
 // parallel.
 #pragma once
 
+#include <algorithm>
+
 #include "das_kernels.cuh"
 #include "launchers.h"
 
@@ -92,36 +94,77 @@ static cudaError_t plain_iq(const PlainParams &p, cudaStream_t st)
 
 namespace rcabf {
 
-template <int KIND, int FB, int STORE, int D>
+// Resident CTAs per SM of a kernel that allocates tensor memory, from its
+// registers, shared memory and TMEM columns.  (For the voxel-blocked kernel
+// with TMEM accumulators the runtime's occupancy query answered one CTA per
+// SM where its registers allowed three.)
+template <typename K>
+static cudaError_t tmem_kernel_occupancy(K k, int threads, size_t smem, int cols, int *occ)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k);
+    if (e != cudaSuccess) return e;
+    int dev = 0, regs_sm = 0, smem_sm = 0, thr_sm = 0, blk_sm = 0, smem_res = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    const int warps = (threads + 31) / 32;
+    const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;   // allocated per warp, 256 at a time
+    const size_t smem_cta = (smem + fa.sharedSizeBytes + smem_res + 127) / 128 * 128;
+    int n = std::min(blk_sm, thr_sm / (warps * 32));
+    n = std::min(n, regs_warp > 0 ? regs_sm / regs_warp / warps : n);
+    n = std::min(n, (int)((size_t)smem_sm / smem_cta));
+    n = std::min(n, 512 / cols);
+    *occ = std::max(n, 0);
+    return cudaSuccess;
+}
+
+template <int KIND, int FB, int STORE, int D, bool TM>
 static cudaError_t vb_do(const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
 {
-    auto k = fused_vb_kernel<KIND, FB, STORE, D>;
+    auto k = fused_vb_kernel<KIND, FB, STORE, D, TM>;
     if (what == 1) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (what == 2) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, VB_THREADS, smem);
+    if (what == 2) {
+        if constexpr (TM) return tmem_kernel_occupancy(k, VB_THREADS, smem, vb_tmem_cols_host(FB), occ);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, VB_THREADS, smem);
+    }
     k<<<grid, VB_THREADS, smem, st>>>(*p);
     return cudaGetLastError();
 }
 
+// tm: accumulators in tensor memory (frame blocks of 8 and 16 only, where
+// they take 64 / 128 registers otherwise)
 template <int KIND, int STORE, int D>
-static cudaError_t vb_fb(int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what, int *occ)
+static cudaError_t vb_fb(int tm, int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what,
+                         int *occ)
 {
+    if (tm) {
+        switch (fb) {
+        case 8: return vb_do<KIND, 8, STORE, D, true>(p, grid, smem, st, what, occ);
+        case 16: return vb_do<KIND, 16, STORE, D, true>(p, grid, smem, st, what, occ);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (fb) {
-    case 2: return vb_do<KIND, 2, STORE, D>(p, grid, smem, st, what, occ);
-    case 4: return vb_do<KIND, 4, STORE, D>(p, grid, smem, st, what, occ);
-    case 8: return vb_do<KIND, 8, STORE, D>(p, grid, smem, st, what, occ);
-    case 16: return vb_do<KIND, 16, STORE, D>(p, grid, smem, st, what, occ);
+    case 2: return vb_do<KIND, 2, STORE, D, false>(p, grid, smem, st, what, occ);
+    case 4: return vb_do<KIND, 4, STORE, D, false>(p, grid, smem, st, what, occ);
+    case 8: return vb_do<KIND, 8, STORE, D, false>(p, grid, smem, st, what, occ);
+    case 16: return vb_do<KIND, 16, STORE, D, false>(p, grid, smem, st, what, occ);
     default: return cudaErrorInvalidValue;
     }
 }
 
 template <int KIND, int D>
-static cudaError_t vb_store(int store, int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st,
-                            int what, int *occ)
+static cudaError_t vb_store(int tm, int store, int fb, const FusedParams *p, int grid, size_t smem,
+                            cudaStream_t st, int what, int *occ)
 {
     switch (store) {
-    case ST_F32: return vb_fb<KIND, ST_F32, D>(fb, p, grid, smem, st, what, occ);
-    case ST_F16: return vb_fb<KIND, ST_F16, D>(fb, p, grid, smem, st, what, occ);
-    case ST_BF16: return vb_fb<KIND, ST_BF16, D>(fb, p, grid, smem, st, what, occ);
+    case ST_F32: return vb_fb<KIND, ST_F32, D>(tm, fb, p, grid, smem, st, what, occ);
+    case ST_F16: return vb_fb<KIND, ST_F16, D>(tm, fb, p, grid, smem, st, what, occ);
+    case ST_BF16: return vb_fb<KIND, ST_BF16, D>(tm, fb, p, grid, smem, st, what, occ);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -130,11 +173,11 @@ static cudaError_t vb_store(int store, int fb, const FusedParams *p, int grid, s
 
 #define RCABF_VB_TU(KIND, NAME)                                                                      \
     namespace rcabf {                                                                                \
-    cudaError_t vb_entry_##NAME(int d, int store, int fb, const FusedParams *p, int grid, size_t smem,\
-                                cudaStream_t st, int what, int *occ)                                 \
+    cudaError_t vb_entry_##NAME(int d, int tm, int store, int fb, const FusedParams *p, int grid,    \
+                                size_t smem, cudaStream_t st, int what, int *occ)                    \
     {                                                                                                \
-        if (d == 1) return vb_store<KIND, 1>(store, fb, p, grid, smem, st, what, occ);               \
-        if (d == 2) return vb_store<KIND, 2>(store, fb, p, grid, smem, st, what, occ);               \
+        if (d == 1) return vb_store<KIND, 1>(tm, store, fb, p, grid, smem, st, what, occ);           \
+        if (d == 2) return vb_store<KIND, 2>(tm, store, fb, p, grid, smem, st, what, occ);           \
         return cudaErrorInvalidValue;                                                                \
     }                                                                                                \
     }

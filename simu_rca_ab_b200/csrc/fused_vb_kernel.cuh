@@ -21,9 +21,21 @@
 // of the record are zero-filled, so no load needs clamping.  The
 // interpolation weights come from degree-8 polynomials (weight_poly.h),
 // each mirrored pair of taps from one even and one odd chain.
+//
+// TM variant: the 2 x VB x FB accumulator words of a thread (128 at FB = 16,
+// half the register file a thread can have) live in tensor memory instead
+// of registers.  Per frame pair the warp loads the 16 words of the pair
+// (VB voxels x 2 frames x re/im) from its own TMEM lanes, adds the step's
+// terms and stores them back; a thread then fits in 128 registers instead of
+// 255 (with spills), so four CTAs share an SM (16 warps instead of 8, all 512
+// TMEM columns at FB = 16) to hide the shared-memory and FMA latencies.  TMEM loads and stores are warp-collective, so
+// the accumulation runs for the whole warp whenever one of its lanes has a
+// contribution; lanes without one keep their words unchanged (a select, so
+// whatever their clamped rows hold never reaches the sums).
 #pragma once
 
 #include "das_common.cuh"
+#include "tmem.cuh"
 #include "weight_poly.h"
 
 namespace rcabf {
@@ -132,11 +144,63 @@ __device__ __forceinline__ VbWindow vb_window(const FusedJob &J, const VbRanges 
     return w;
 }
 
-template <int KIND, int FB, int STORE, int D>
-__global__ void __launch_bounds__(VB_THREADS, VB_MIN_BLOCKS)
+// Weights of each voxel shifted to its first row within the block's rows
+// (zeros elsewhere and for voxels without a contribution) and its complex
+// factor P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab).
+template <int KIND, int D>
+__device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&fl)[VB], const float (&dd)[VB],
+                                         bool (&ok)[VB], float base, const float (&txr)[VB],
+                                         const float (&txq)[VB], float4 e, float2 abp,
+                                         float (&ws)[VB][KindTraits<KIND>::TAPS + D], float2 (&P)[VB])
+{
+    constexpr int TAPS = KindTraits<KIND>::TAPS;
+    constexpr int R = TAPS + D;
+#pragma unroll
+    for (int v = 0; v < VB; ++v) {
+        int o = (int)(fl[v] - base);
+        if (ok[v] && o > D) { atomicAdd(prm.err_count, 1ull); ok[v] = false; }
+        o = ok[v] ? o : 0;
+        float w[TAPS];
+        poly_weights<KIND>(dd[v], w);
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            float a = (k < TAPS) ? w[k] : 0.0f;
+            if constexpr (D >= 1) { if (o == 1) a = (k >= 1 && k - 1 < TAPS) ? w[k - 1] : 0.0f; }
+            if constexpr (D >= 2) { if (o == 2) a = (k >= 2 && k - 2 < TAPS) ? w[k - 2] : 0.0f; }
+            ws[v][k] = ok[v] ? a : 0.0f;
+        }
+        const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
+        P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
+                     : make_float2(0.f, 0.f);
+    }
+}
+
+// Weighted row sums of one frame pair for every voxel: ts[v] = sum_k
+// ws[v][k] * row k (re, im of frame 2p; re, im of frame 2p + 1).
+template <int R, int STRIDE>
+__device__ __forceinline__ void vb_pair_sums(const char *rows, const float (&ws)[VB][R], float4 (&ts)[VB])
+{
+#pragma unroll
+    for (int v = 0; v < VB; ++v) ts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const float4 x = *reinterpret_cast<const float4 *>(rows + k * STRIDE);
+#pragma unroll
+        for (int v = 0; v < VB; ++v) {
+            ts[v].x = fmaf(ws[v][k], x.x, ts[v].x);
+            ts[v].y = fmaf(ws[v][k], x.y, ts[v].y);
+            ts[v].z = fmaf(ws[v][k], x.z, ts[v].z);
+            ts[v].w = fmaf(ws[v][k], x.w, ts[v].w);
+        }
+    }
+}
+
+template <int KIND, int FB, int STORE, int D, bool TM>
+__global__ void __launch_bounds__(VB_THREADS, TM ? VB_TM_MIN_BLOCKS : VB_MIN_BLOCKS)
 fused_vb_kernel(const __grid_constant__ FusedParams prm)
 {
     static_assert(FB % 2 == 0, "frames are processed in pairs");
+    static_assert(!TM || VB == 4, "a TMEM access moves the 16 words of VB = 4 voxels x one frame pair");
     using T = typename StoreT<STORE>::T;
     using KT = KindTraits<KIND>;
     constexpr int TAPS = KT::TAPS;
@@ -158,13 +222,31 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
     {
         unsigned dyn;
         asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        // (TM: lanes without a contribution read R rows of a stage, so a
+        // stage holds at least R)
         if (dyn < (unsigned)(NST * stage_bytes) || prm.row_words * 4 != STRIDE ||
-            (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS)) {
+            (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS) || (TM && prm.wmax < R)) {
             if (tid == 0) atomicAdd(prm.err_count, 1ull);
             return;
         }
     }
     unsigned char *stages = smem;
+
+    // TM: warp 0 allocates the CTA's columns; each warp addresses the 32
+    // lanes of its quadrant, each thread its own lane
+    constexpr uint32_t TCOLS = (uint32_t)vb_tmem_cols_host(FB);
+    uint32_t tlane = 0;
+    if constexpr (TM) {
+        __shared__ uint32_t tbase;
+        if (tid < 32) {
+            tmem_alloc(&tbase, TCOLS);
+            tmem_relinquish();
+        }
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        tlane = tbase + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16);
+    }
 
     for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x) {
         int ji = 0;
@@ -198,6 +280,55 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         for (int v = 0; v < VB; ++v)
 #pragma unroll
             for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
+        // TM: words [16 p, 16 p + 16) of a lane hold frames 2p, 2p + 1 of
+        // its voxels: voxel v at 4 v + {re 2p, im 2p, re 2p+1, im 2p+1}
+        auto tm_zero = [&]() {
+            uint32_t z[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[i] = 0u;
+            __syncwarp();   // TMEM accesses are warp-collective: converge first
+#pragma unroll
+            for (int c = 0; c < FB; c += 2) tmem_st16(tlane + (uint32_t)(c * 8), z);
+        };
+        // per-voxel, per-frame output of the accumulators (TM: read back
+        // from the lane's words), optionally added to what `out` holds
+        auto emit = [&](int64_t frame_stride, int64_t frame_off) {
+#pragma unroll
+            for (int c = 0; c < FB; c += 2) {
+                float2 a[VB][2];
+                if constexpr (TM) {
+                    uint32_t w[16];
+                    __syncwarp();
+                    tmem_wait_st();
+                    tmem_ld16(tlane + (uint32_t)(c * 8), w);
+                    tmem_wait_ld16(w);
+#pragma unroll
+                    for (int v = 0; v < VB; ++v) {
+                        a[v][0] = make_float2(__uint_as_float(w[4 * v]), __uint_as_float(w[4 * v + 1]));
+                        a[v][1] = make_float2(__uint_as_float(w[4 * v + 2]), __uint_as_float(w[4 * v + 3]));
+                    }
+                } else {
+#pragma unroll
+                    for (int v = 0; v < VB; ++v) { a[v][0] = acc[v][c]; a[v][1] = acc[v][c + 1]; }
+                }
+#pragma unroll
+                for (int v = 0; v < VB; ++v) {
+                    if (v < nvv) {
+                        const int64_t pix = iz * g.s_z + iu * g.s_u + (iv0 + v) * g.s_v;
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int fr = fb * FB + c + h;
+                            if (fr < J.n_frame) {
+                                float2 *o = J.out + (int64_t)fr * frame_stride + frame_off + pix;
+                                if (J.accumulate) { float2 q = *o; q.x += a[v][h].x; q.y += a[v][h].y; *o = q; }
+                                else *o = a[v][h];
+                            }
+                        }
+                    }
+                }
+            }
+        };
+        if constexpr (TM) tm_zero();
 
         auto slab = [&](int tx, int rx) -> const char * {
             return S + (((int64_t)tx * g.n_ele + rx) * J.n_fb + fb) * J.slab_bytes;
@@ -311,10 +442,55 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                 }
             }
 
-            if (!wA.skip && cone_bits != 0 && e.w > 0.0f) {
+            if constexpr (!TM) {
+                if (!wA.skip && cone_bits != 0 && e.w > 0.0f) {
+                    const float ab = ab_value(g, tx, rx);
+                    const float2 abp = ab_phasor(g, tx, rx);
+                    // sample index of each voxel; rows are shared from the lowest
+                    float fl[VB], dd[VB];
+                    bool ok[VB];
+                    float base = 3.0e38f;
+#pragma unroll
+                    for (int v = 0; v < VB; ++v) {
+                        const float idx = __fadd_rn(__fadd_rn(txi[v], e.x), ab);
+                        fl[v] = floorf(idx);
+                        dd[v] = idx - fl[v];
+                        ok[v] = ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
+                                fl[v] < (float)(J.n_sample - 1 - KT::HI);
+                        if (ok[v]) base = fminf(base, fl[v]);
+                    }
+                    if (base < 2.0e38f) {
+                        float ws[VB][R];
+                        float2 P[VB];
+                        vb_terms<KIND, D>(prm, fl, dd, ok, base, txr, txq, e, abp, ws, P);
+                        const int row0 = (int)base - KT::LO - wA.lo;
+                        if (row0 < 0 || row0 + R > wA.count || wA.overflow) {
+                            atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
+                        } else {
+                            const char *rows = reinterpret_cast<const char *>(stages) +
+                                               (s % NST) * stage_bytes + row0 * STRIDE;
+#pragma unroll
+                            for (int c = 0; c < FB; c += 2) {
+                                float4 ts[VB];
+                                vb_pair_sums<R, STRIDE>(rows + c * 8, ws, ts);
+#pragma unroll
+                                for (int v = 0; v < VB; ++v) {
+                                    float2 &a0 = acc[v][c], &a1 = acc[v][c + 1];
+                                    a0.x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0.x));
+                                    a0.y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0.y));
+                                    a1.x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1.x));
+                                    a1.y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1.y));
+                                }
+                            }
+                        }
+                    }
+                }
+            } else {
+                // every lane computes its terms (lanes without voxels carry
+                // zeros); the warp accumulates when any lane contributes
+                const bool act = !wA.skip && cone_bits != 0 && e.w > 0.0f;
                 const float ab = ab_value(g, tx, rx);
                 const float2 abp = ab_phasor(g, tx, rx);
-                // sample index of each voxel; rows are shared from the lowest
                 float fl[VB], dd[VB];
                 bool ok[VB];
                 float base = 3.0e38f;
@@ -323,87 +499,63 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     const float idx = __fadd_rn(__fadd_rn(txi[v], e.x), ab);
                     fl[v] = floorf(idx);
                     dd[v] = idx - fl[v];
-                    ok[v] = ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
+                    ok[v] = act && ((cone_bits >> v) & 1u) && fl[v] >= (float)KT::LO &&
                             fl[v] < (float)(J.n_sample - 1 - KT::HI);
                     if (ok[v]) base = fminf(base, fl[v]);
                 }
-                if (base < 2.0e38f) {
+                bool use = base < 2.0e38f;
+                int row0 = use ? (int)base - KT::LO - wA.lo : 0;
+                if (use && (row0 < 0 || row0 + R > wA.count || wA.overflow)) {
+                    atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
+                    use = false;
+                }
+                if (!use) {   // rows [0, R) of the stage exist (wmax >= R); all weights zero
+                    row0 = 0;
+#pragma unroll
+                    for (int v = 0; v < VB; ++v) ok[v] = false;
+                }
+                if (__any_sync(0xffffffffu, use)) {
                     float ws[VB][R];
                     float2 P[VB];
-                    int omax = 0;
+                    vb_terms<KIND, D>(prm, fl, dd, ok, use ? base : 0.0f, txr, txq, e, abp, ws, P);
+                    const char *rows = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes +
+                                       row0 * STRIDE;
+                    __syncwarp();     // converged after the divergent checks above
+                    tmem_wait_st();   // the previous step's stores are visible to the loads below
 #pragma unroll
-                    for (int v = 0; v < VB; ++v) {
-                        int o = (int)(fl[v] - base);
-                        if (ok[v] && o > D) { atomicAdd(prm.err_count, 1ull); ok[v] = false; }
-                        o = ok[v] ? o : 0;
-                        omax = max(omax, o);
-                        float w[TAPS];
-                        poly_weights<KIND>(dd[v], w);
+                    for (int c = 0; c < FB; c += 2) {
+                        uint32_t w[16];
+                        tmem_ld16(tlane + (uint32_t)(c * 8), w);
+                        float4 ts[VB];
+                        vb_pair_sums<R, STRIDE>(rows + c * 8, ws, ts);
+                        tmem_wait_ld16(w);
 #pragma unroll
-                        for (int k = 0; k < R; ++k) {
-                            float a = (k < TAPS) ? w[k] : 0.0f;
-                            if constexpr (D >= 1) { if (o == 1) a = (k >= 1 && k - 1 < TAPS) ? w[k - 1] : 0.0f; }
-                            if constexpr (D >= 2) { if (o == 2) a = (k >= 2 && k - 2 < TAPS) ? w[k - 2] : 0.0f; }
-                            ws[v][k] = ok[v] ? a : 0.0f;
+                        for (int v = 0; v < VB; ++v) {
+                            const float a0x = __uint_as_float(w[4 * v]), a0y = __uint_as_float(w[4 * v + 1]);
+                            const float a1x = __uint_as_float(w[4 * v + 2]), a1y = __uint_as_float(w[4 * v + 3]);
+                            const float n0x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0x));
+                            const float n0y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0y));
+                            const float n1x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1x));
+                            const float n1y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1y));
+                            w[4 * v] = use ? __float_as_uint(n0x) : w[4 * v];
+                            w[4 * v + 1] = use ? __float_as_uint(n0y) : w[4 * v + 1];
+                            w[4 * v + 2] = use ? __float_as_uint(n1x) : w[4 * v + 2];
+                            w[4 * v + 3] = use ? __float_as_uint(n1y) : w[4 * v + 3];
                         }
-                        // P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab)
-                        const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
-                        P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
-                                     : make_float2(0.f, 0.f);
-                    }
-                    const int row0 = (int)base - KT::LO - wA.lo;
-                    if (row0 < 0 || row0 + R > wA.count || wA.overflow) {
-                        atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
-                    } else {
-                        const char *rows = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes +
-                                           row0 * STRIDE;
-#pragma unroll
-                        for (int c = 0; c < FB; c += 2) {
-                            float4 ts[VB];
-#pragma unroll
-                            for (int v = 0; v < VB; ++v) ts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-                            for (int k = 0; k < R; ++k) {
-                                const float4 x = *reinterpret_cast<const float4 *>(rows + k * STRIDE + c * 8);
-#pragma unroll
-                                for (int v = 0; v < VB; ++v) {
-                                    ts[v].x = fmaf(ws[v][k], x.x, ts[v].x);
-                                    ts[v].y = fmaf(ws[v][k], x.y, ts[v].y);
-                                    ts[v].z = fmaf(ws[v][k], x.z, ts[v].z);
-                                    ts[v].w = fmaf(ws[v][k], x.w, ts[v].w);
-                                }
-                            }
-#pragma unroll
-                            for (int v = 0; v < VB; ++v) {
-                                float2 &a0 = acc[v][c], &a1 = acc[v][c + 1];
-                                a0.x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0.x));
-                                a0.y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0.y));
-                                a1.x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1.x));
-                                a1.y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1.y));
-                            }
-                        }
-                        (void)omax;
+                        tmem_st16(tlane + (uint32_t)(c * 8), w);
                     }
                 }
             }
 
             if (rx == g.n_ele - 1 && !J.compound) {   // per-transmit output
+                emit((int64_t)g.n_tx * g.n_pix, (int64_t)tx * g.n_pix);
+                if constexpr (TM) {
+                    tm_zero();
+                } else {
 #pragma unroll
-                for (int v = 0; v < VB; ++v) {
-                    if (v < nvv) {
-                        const int64_t pix = iz * g.s_z + iu * g.s_u + (iv0 + v) * g.s_v;
+                    for (int v = 0; v < VB; ++v)
 #pragma unroll
-                        for (int f = 0; f < FB; ++f) {
-                            const int fr = fb * FB + f;
-                            if (fr < J.n_frame) {
-                                float2 *o = J.out + ((int64_t)fr * g.n_tx + tx) * g.n_pix + pix;
-                                if (J.accumulate) { float2 q = *o; q.x += acc[v][f].x; q.y += acc[v][f].y; *o = q; }
-                                else *o = acc[v][f];
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
+                        for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
                 }
             }
 
@@ -420,22 +572,17 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         if constexpr (ASYNC) cp_async_wait<0>();
         __syncthreads();
 
-        if (J.compound) {
-#pragma unroll
-            for (int v = 0; v < VB; ++v) {
-                if (v < nvv) {
-                    const int64_t pix = iz * g.s_z + iu * g.s_u + (iv0 + v) * g.s_v;
-#pragma unroll
-                    for (int f = 0; f < FB; ++f) {
-                        const int fr = fb * FB + f;
-                        if (fr < J.n_frame) {
-                            float2 *o = J.out + (int64_t)fr * g.n_pix + pix;
-                            if (J.accumulate) { float2 q = *o; q.x += acc[v][f].x; q.y += acc[v][f].y; *o = q; }
-                            else *o = acc[v][f];
-                        }
-                    }
-                }
-            }
+        if (J.compound) emit(g.n_pix, 0);
+    }
+    if constexpr (TM) {
+        // every load was waited for; the last stores complete before the free
+        __syncwarp();
+        tmem_wait_st();
+        tmem_fence_before_sync();
+        __syncthreads();
+        if (tid < 32) {
+            tmem_fence_after_sync();
+            tmem_dealloc(tlane, TCOLS);   // warp 0's lane address is the allocation's base
         }
     }
 }

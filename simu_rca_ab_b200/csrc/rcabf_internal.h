@@ -95,6 +95,10 @@ constexpr int VB_BLOCK = 4;          // voxels per thread along v in the voxel-b
 constexpr int VB_THREADS_HOST = 128; // its CTA size
 constexpr int VB_STAGE_REGS = 2;     // 16-byte staging chunks a thread holds (FP16/BF16 slabs)
 constexpr int VB_MIN_BLOCKS = 1;     // launch-bounds hint: more forces spills (~230 registers live)
+constexpr int VB_TM_MIN_BLOCKS = 4;  // the same with the accumulators in tensor memory (128 registers, no spills)
+// tensor-memory columns a CTA of the voxel-blocked kernel allocates: 16 per
+// frame pair, a power of two >= 32
+constexpr RCABF_HD int vb_tmem_cols_host(int fb) { return fb * 8 <= 32 ? 32 : fb * 8; }
 
 struct FusedParams {
     FusedJob jobs[MAX_JOBS];

@@ -263,7 +263,7 @@ def test_voxel_blocked_kernel_vs_fp64_on_c2_geometry(bf, c2_small, storage, tol)
     from simu_rca_ab_b200 import workloads as W
     w, data = c2_small
     out, plan = _beamform_dev(bf, w, data, storage, "fused")
-    assert plan["kernel"] == "fused_voxel_blocked", plan
+    assert plan["kernel"].startswith("fused_voxel_blocked"), plan
     rng = np.random.default_rng(7)
     pix = np.sort(rng.choice(out.shape[1], 1024, replace=False))
     dn = data.cpu().numpy()
@@ -354,7 +354,7 @@ def test_autotune_keeps_the_fastest_choice_and_the_result(bf, c2_small):
     plan1 = eng.plan(geom, a3)
     assert plan1["frames_per_block"] == res["frames_per_block"]
     assert plan1["tile"] == [res["tile_u"], res["tile_v"], res["tile_z"]]
-    assert plan1["kernel"] == ("fused_voxel_blocked" if res["voxel_blocked"] else "fused")
+    assert plan1["kernel"] == {0: "fused", 1: "fused_voxel_blocked", 2: "fused_voxel_blocked_tmem"}[res["voxel_blocked"]]
     eng.run(geom, a3)
     torch.cuda.synchronize()
     assert H.rel_rms(after.cpu().numpy(), before.cpu().numpy()) < 1e-4
