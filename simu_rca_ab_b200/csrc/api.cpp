@@ -198,9 +198,6 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
             }
             const int need = (int)std::min<int64_t>(
                 g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
-            // rows a stage holds: the window, and with tensor-memory
-            // accumulators at least the taps + shift rows every lane reads
-            auto rows_for = [&](int tm) { return tm ? std::max(need, kind_taps(g->kind) + d) : need; };
             auto pick_fb = [&](int tm) {   // the largest frame block whose window fits
                 for (int c : {16, 8, 4, 2}) {
                     if (tm && c < 8) continue;
@@ -210,7 +207,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
                     const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
                                                                            fused_row_words(c) * 4)),
                                                   vb_stage_rows_cap(p.store, c));
-                    if (cap >= rows_for(tm)) return c;
+                    if (cap >= need) return c;
                 }
                 return 0;
             };
@@ -223,8 +220,8 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
                 p.fb = fb;
                 p.ts = vts;
                 layout(vts.tv * VB_BLOCK);
-                p.wmax = rows_for(tm);
-                p.smem = vb_smem_bytes(p.store, p.wmax, p.row_words);
+                p.wmax = need;
+                p.smem = vb_smem_bytes(p.store, p.wmax, p.row_words, tm ? kind_taps(g->kind) + d : 0);
                 return RCABF_OK;
             }
         }
@@ -325,7 +322,8 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     // a counter set by the caller (rcabf_beamform_noalloc) is kept
     DeviceState *ds = device_state(g0->device, prm.err_count == nullptr);
     if (!prm.err_count) prm.err_count = ds->err;
-    const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words)
+    const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words,
+                                             p.vb == 2 ? kind_taps(g0->kind) + p.d : 0)
                              : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
     int occ = 0;
     const int so = resident_ctas(g0, p, smem, ds, occ);

@@ -30,8 +30,8 @@
 // 255 (with spills), so four CTAs share an SM (16 warps instead of 8, all 512
 // TMEM columns at FB = 16) to hide the shared-memory and FMA latencies.  TMEM loads and stores are warp-collective, so
 // the accumulation runs for the whole warp whenever one of its lanes has a
-// contribution; lanes without one keep their words unchanged (a select, so
-// whatever their clamped rows hold never reaches the sums).
+// contribution; lanes without one read R rows of zeros kept in shared memory
+// with zero weights, so they add exact zeros.
 #pragma once
 
 #include "das_common.cuh"
@@ -222,10 +222,9 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
     {
         unsigned dyn;
         asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-        // (TM: lanes without a contribution read R rows of a stage, so a
-        // stage holds at least R)
-        if (dyn < (unsigned)(NST * stage_bytes) || prm.row_words * 4 != STRIDE ||
-            (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS) || (TM && prm.wmax < R)) {
+        // (TM: R rows of zeros follow the stages)
+        if (dyn < (unsigned)(NST * stage_bytes + (TM ? R * STRIDE : 0)) || prm.row_words * 4 != STRIDE ||
+            (!ASYNC && prm.wmax * CPR > SREGS * VB_THREADS)) {
             if (tid == 0) atomicAdd(prm.err_count, 1ull);
             return;
         }
@@ -236,8 +235,11 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
     // lanes of its quadrant, each thread its own lane
     constexpr uint32_t TCOLS = (uint32_t)vb_tmem_cols_host(FB);
     uint32_t tlane = 0;
+    const int zero_off = NST * stage_bytes;   // TM: offset of R staged rows of zeros
     if constexpr (TM) {
         __shared__ uint32_t tbase;
+        for (int i = tid; i < R * STRIDE / 16; i += VB_THREADS)
+            *reinterpret_cast<float4 *>(smem + zero_off + 16 * i) = make_float4(0.f, 0.f, 0.f, 0.f);
         if (tid < 32) {
             tmem_alloc(&tbase, TCOLS);
             tmem_relinquish();
@@ -509,8 +511,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
                     use = false;
                 }
-                if (!use) {   // rows [0, R) of the stage exist (wmax >= R); all weights zero
-                    row0 = 0;
+                if (!use) {   // all weights zero, rows of zeros: the lane adds exact zeros
 #pragma unroll
                     for (int v = 0; v < VB; ++v) ok[v] = false;
                 }
@@ -518,11 +519,13 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     float ws[VB][R];
                     float2 P[VB];
                     vb_terms<KIND, D>(prm, fl, dd, ok, use ? base : 0.0f, txr, txq, e, abp, ws, P);
-                    const char *rows = reinterpret_cast<const char *>(stages) + (s % NST) * stage_bytes +
-                                       row0 * STRIDE;
+                    const char *rows = reinterpret_cast<const char *>(stages) +
+                                       (use ? (s % NST) * stage_bytes + row0 * STRIDE : zero_off);
                     __syncwarp();     // converged after the divergent checks above
                     tmem_wait_st();   // the previous step's stores are visible to the loads below
-#pragma unroll
+                    // (not unrolled: an unrolled loop spills at 128 registers and
+                    // measured 14% slower)
+#pragma unroll 1
                     for (int c = 0; c < FB; c += 2) {
                         uint32_t w[16];
                         tmem_ld16(tlane + (uint32_t)(c * 8), w);
@@ -537,10 +540,10 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                             const float n0y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0y));
                             const float n1x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1x));
                             const float n1y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1y));
-                            w[4 * v] = use ? __float_as_uint(n0x) : w[4 * v];
-                            w[4 * v + 1] = use ? __float_as_uint(n0y) : w[4 * v + 1];
-                            w[4 * v + 2] = use ? __float_as_uint(n1x) : w[4 * v + 2];
-                            w[4 * v + 3] = use ? __float_as_uint(n1y) : w[4 * v + 3];
+                            w[4 * v] = __float_as_uint(n0x);
+                            w[4 * v + 1] = __float_as_uint(n0y);
+                            w[4 * v + 2] = __float_as_uint(n1x);
+                            w[4 * v + 3] = __float_as_uint(n1y);
                         }
                         tmem_st16(tlane + (uint32_t)(c * 8), w);
                     }

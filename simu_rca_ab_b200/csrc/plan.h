@@ -50,9 +50,11 @@ constexpr size_t VB_SMEM_BUDGET = 72 * 1024;
 // 1: the planner gives the voxel-blocked kernel tensor-memory accumulators
 // where the frame block allows (8 or 16 frames), 0: registers
 constexpr int VB_TMEM_DEFAULT = 1;
-inline size_t vb_smem_bytes(int store, int wmax, int row_words)
+// (with tensor-memory accumulators, vb = 2, followed by `zero_rows` staged
+// rows of zeros that lanes without a contribution read)
+inline size_t vb_smem_bytes(int store, int wmax, int row_words, int zero_rows = 0)
 {
-    return (size_t)fused_stages(store) * wmax * row_words * 4;
+    return (size_t)(fused_stages(store) * wmax + zero_rows) * row_words * 4;
 }
 inline int vb_stage_rows_cap(int store, int fb)
 {
