@@ -104,14 +104,15 @@ struct VbRanges {
     float ab;        // aberration delay of the step
 };
 
-__device__ __forceinline__ VbRanges vb_ranges(const FusedJob &J, int s, int n_steps, int tu, int tv, int tz)
+// step s = tx * n_ele + rx
+__device__ __forceinline__ VbRanges vb_ranges(const FusedJob &J, int s, int n_steps, int tx, int rx, int tu, int tv,
+                                              int tz)
 {
     VbRanges r;
     if (s >= n_steps) {   // past the last step: an empty range (skipped)
         r.rr = make_float2(1.0f, 0.0f); r.tr = r.rr; r.ab = 0.0f;
         return r;
     }
-    const int tx = s / J.g.n_ele, rx = s % J.g.n_ele;
     r.rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
     r.tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
     r.ab = ab_value(J.g, tx, rx);
@@ -145,8 +146,9 @@ __device__ __forceinline__ VbWindow vb_window(const FusedJob &J, const VbRanges 
 }
 
 // Weights of each voxel shifted to its first row within the block's rows
-// (zeros elsewhere and for voxels without a contribution) and its complex
-// factor P = apod * exp(j phase_tx) * exp(j phase_rx) * exp(j phase_ab).
+// (zeros elsewhere) and its complex factor P = apod * exp(j phase_tx) *
+// exp(j phase_rx) * exp(j phase_ab), zero for a voxel without a contribution
+// (its weights then multiply finite staged rows into an exact zero).
 template <int KIND, int D>
 __device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&fl)[VB], const float (&dd)[VB],
                                          bool (&ok)[VB], float base, const float (&txr)[VB],
@@ -161,13 +163,13 @@ __device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&f
         if (ok[v] && o > D) { atomicAdd(prm.err_count, 1ull); ok[v] = false; }
         o = ok[v] ? o : 0;
         float w[TAPS];
-        poly_weights<KIND>(dd[v], w);
+        poly_weights<KIND>(ok[v] ? dd[v] : 0.0f, w);   // finite whatever the index of a masked voxel
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             float a = (k < TAPS) ? w[k] : 0.0f;
             if constexpr (D >= 1) { if (o == 1) a = (k >= 1 && k - 1 < TAPS) ? w[k - 1] : 0.0f; }
             if constexpr (D >= 2) { if (o == 2) a = (k >= 2 && k - 2 < TAPS) ? w[k - 2] : 0.0f; }
-            ws[v][k] = ok[v] ? a : 0.0f;
+            ws[v][k] = a;   // finite; a voxel without a contribution has P = 0
         }
         const float qx = fmaf(txr[v], e.y, -txq[v] * e.z), qy = fmaf(txr[v], e.z, txq[v] * e.y);
         P[v] = ok[v] ? make_float2(fmaf(qx, abp.x, -qy * abp.y), fmaf(qx, abp.y, qy * abp.x))
@@ -332,14 +334,18 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
         if constexpr (TM) tm_zero();
 
-        auto slab = [&](int tx, int rx) -> const char * {
-            return S + (((int64_t)tx * g.n_ele + rx) * J.n_fb + fb) * J.slab_bytes;
+        // slabs are ordered by step s = tx * n_ele + rx, then frame block
+        auto slab = [&](int s) -> const char * { return S + ((int64_t)s * J.n_fb + fb) * J.slab_bytes; };
+        // (tx, rx) of step s: divided once per item, then advanced per step
+        auto advance = [&](int &tx, int &rx) {
+            if (++rx == g.n_ele) { rx = 0; ++tx; }
         };
         auto window = [&](int s) -> VbWindow {
             VbWindow w;
             w.skip = true; w.lo = 0; w.count = 0; w.data = 0; w.overflow = false;
             if (s >= n_steps) return w;
-            return vb_window<KIND, D>(J, vb_ranges(J, s, n_steps, tu, tv, tz), prm.wmax);
+            return vb_window<KIND, D>(J, vb_ranges(J, s, n_steps, s / g.n_ele, s % g.n_ele, tu, tv, tz),
+                                      prm.wmax);
         };
         // rows [data, count) of a staged buffer hold zeros (shift rows past the record)
         auto zero_tail = [&](unsigned char *dst, const VbWindow &w) {
@@ -351,7 +357,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
         auto issue_async = [&](int s, const VbWindow &w) {
             if (!w.skip && !w.overflow) {
-                const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
+                const char *src = slab(s) + (int64_t)w.lo * RAWB;
                 unsigned char *dst = stages + (s % NST) * stage_bytes;
                 const int nch = w.data * CPR;
                 for (int c = tid; c < nch; c += VB_THREADS) {
@@ -365,7 +371,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         Chunk regs[SREGS];
         auto load_regs = [&](int s, const VbWindow &w) {
             if (w.skip || w.overflow) return;
-            const char *src = slab(s / g.n_ele, s % g.n_ele) + (int64_t)w.lo * RAWB;
+            const char *src = slab(s) + (int64_t)w.lo * RAWB;
             const int nch = w.data * CPR;
 #pragma unroll
             for (int k = 0; k < SREGS; ++k) {
@@ -400,7 +406,9 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
 
         VbWindow wA = window(0), wB = window(1), wC;
-        VbRanges rnext = vb_ranges(J, 2, n_steps, tu, tv, tz);   // ranges of the step two ahead
+        int tx3 = 2 / g.n_ele, rx3 = 2 % g.n_ele;   // step of the ranges loaded next
+        VbRanges rnext = vb_ranges(J, 2, n_steps, tx3, rx3, tu, tv, tz);   // ranges of the step two ahead
+        advance(tx3, rx3);
         if constexpr (ASYNC) {
             issue_async(0, wA);
             issue_async(1, wB);
@@ -418,18 +426,19 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         for (int v = 0; v < VB; ++v) { txi[v] = 0.f; txr[v] = 0.f; txq[v] = 0.f; }
         float4 enext = nvv > 0 ? __ldg(&g.rx_tab[rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
 
-        for (int s = 0; s < n_steps; ++s) {
-            const int tx = s / g.n_ele, rx = s % g.n_ele;
+        int tx = 0, rx = 0;   // of step s
+        for (int s = 0; s < n_steps; ++s, advance(tx, rx)) {
             if constexpr (ASYNC) {
                 cp_async_wait<NST - 2>();
                 __syncthreads();
                 wC = vb_window<KIND, D>(J, rnext, prm.wmax);
-                rnext = vb_ranges(J, s + 3, n_steps, tu, tv, tz);
+                rnext = vb_ranges(J, s + 3, n_steps, tx3, rx3, tu, tv, tz);
+                advance(tx3, rx3);
                 issue_async(s + 2, wC);
             }
             const float4 e = enext;
             if (nvv > 0 && s + 1 < n_steps)
-                enext = __ldg(&g.rx_tab[(int64_t)((s + 1) % g.n_ele) * n_rxkey + rxkey]);
+                enext = __ldg(&g.rx_tab[(int64_t)(rx + 1 == g.n_ele ? 0 : rx + 1) * n_rxkey + rxkey]);
             if (rx == 0 && nvv > 0) {
                 const float4 *txrow = g.tx_tab + (int64_t)tx * n_txkey + iz;
                 cone_bits = 0;
@@ -565,7 +574,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
             if constexpr (!ASYNC) {
                 store_regs(s + 1, wB);
                 wC = vb_window<KIND, D>(J, rnext, prm.wmax);
-                rnext = vb_ranges(J, s + 3, n_steps, tu, tv, tz);
+                rnext = vb_ranges(J, s + 3, n_steps, tx3, rx3, tu, tv, tz);
+                advance(tx3, rx3);
                 load_regs(s + 2, wC);
                 __syncthreads();
             }
