@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="use the planner's launch choice untimed")
     ap.add_argument("--no-clutter", action="store_true", help="skip the SVD clutter filter of the ensemble")
     ap.add_argument("--no-simulator", action="store_true", help="skip the simulator timing")
+    ap.add_argument("--no-ulm", action="store_true", help="skip the ULM super-localisation timing")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
@@ -265,6 +266,60 @@ def serving_leg(eng, dev, n_requests: int, rate_hz: float, seed: int = 3):
                          "how": "plain_das_kernel per request (device time of 2 frames x frames/2), "
                                 "FIFO queue on the same arrival times"},
     }
+
+
+def ulm_leg(dev, seed: int = 11, nz: int = 256, nx: int = 256, nt: int = 400, n_bubbles: int = 48):
+    """ULM super-localisation (simu_rca_ab_b200.ulm, the reference's
+    Python/superloc/superloc.py) on a synthetic 2-D block: nz x nx pixels x
+    nt frames of complex Gaussian microbubble spots (sigma 1.5 px, moving up
+    to 0.4 px per frame) in -30 dB noise, resident on the device; a 9 x 9
+    Gaussian PSF.  Times PsfCorrMap2D + SuperLocFilter (fit 0) on the
+    device, and DensityMappingND of the localisations."""
+    import numpy as np
+    import torch
+
+    from simu_rca_ab_b200 import ulm as U
+    g = torch.Generator(device=dev).manual_seed(seed)
+    rnd = lambda *s: torch.rand(*s, generator=g, device=dev)
+    z0, x0 = 12 + rnd(n_bubbles) * (nz - 24), 12 + rnd(n_bubbles) * (nx - 24)
+    vz, vx = (rnd(n_bubbles) - 0.5) * 0.8, (rnd(n_bubbles) - 0.5) * 0.8
+    amp = (0.5 + rnd(n_bubbles)) * torch.exp(1j * 2 * np.pi * rnd(n_bubbles))
+    zz = torch.arange(nz, device=dev, dtype=torch.float32)[:, None, None]
+    xx = torch.arange(nx, device=dev, dtype=torch.float32)[None, :, None]
+    tt = torch.arange(nt, device=dev, dtype=torch.float32)[None, None, :]
+    iq = torch.zeros((nz, nx, nt), dtype=torch.complex64, device=dev)
+    for b in range(n_bubbles):
+        zc = (z0[b] + vz[b] * tt).remainder(nz)
+        xc = (x0[b] + vx[b] * tt).remainder(nx)
+        iq += amp[b] * torch.exp(-((zz - zc) ** 2 + (xx - xc) ** 2) / (2 * 1.5 ** 2))
+    iq += 0.03 * torch.complex(torch.randn(iq.shape, generator=g, device=dev),
+                               torch.randn(iq.shape, generator=g, device=dev))
+    k = np.arange(9) - 4.0
+    psf = np.exp(-(k[:, None] ** 2 + k[None, :] ** 2) / (2 * 1.5 ** 2)).astype(np.complex64)
+
+    def run():
+        corr = U.PsfCorrMap2D(iq, psf)
+        return U.SuperLocFilter(corr, iq, 5, 5, 0)
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    corr = U.PsfCorrMap2D(iq, psf)
+    e1.record()
+    pos = U.SuperLocFilter(corr, iq, 5, 5, 0)
+    e2.record()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dens = U.DensityMappingND(pos, np.arange(nx * 4) / 4.0, [0.0], np.arange(nz * 4) / 4.0)
+    dens_ms = (time.perf_counter() - t0) * 1e3
+    corr_ms, loc_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    return {"what": f"ULM (superloc.py): PsfCorrMap2D (9x9 PSF) + SuperLocFilter (fit 0) on {nz}x{nx} px x {nt} "
+                    f"frames of {n_bubbles} moving microbubbles in -30 dB noise, device-resident; "
+                    "DensityMappingND at 4x super-resolution (host arrays in and out)",
+            "corr_ms": corr_ms, "superloc_ms": loc_ms, "ms": corr_ms + loc_ms,
+            "frames_per_s": nt / ((corr_ms + loc_ms) / 1e3), "localisations": int(pos.shape[1]),
+            "density_ms": dens_ms, "density_total": float(dens.sum())}
 
 
 def simulator_leg(dev, seed: int = 7):
@@ -601,6 +656,13 @@ def main():
         except Exception as ex:
             sim = {"error": f"{type(ex).__name__}: {ex}"}
 
+    ulm = None
+    if not a.no_ulm and rank == 0:
+        try:
+            ulm = ulm_leg(dev)
+        except Exception as ex:
+            ulm = {"error": f"{type(ex).__name__}: {ex}"}
+
     line = None
     if rank == 0:
         from oracle import host as H
@@ -657,7 +719,7 @@ def main():
                        "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
-            "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim,
+            "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim, "ulm": ulm,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

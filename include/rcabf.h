@@ -363,6 +363,81 @@ int rcabf_sim_element_field(void *out, const float *r_scat, const float *r_ele, 
                             float height, float rfocus, int baffle, float lens, float speed_of_sound,
                             int64_t n_scat, int64_t n_ele, int64_t n_f, int64_t n_sub, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* ULM super-localisation (downstream of the clutter filter)                 */
+/* ------------------------------------------------------------------------ */
+/* Maps are stacks of 2-D frames, device memory, z fastest, then x, then
+ * frame: element (z, x, t) at z + nz * (x + nx * t) -- the column-major
+ * layout of the reference's (Nz, Nx, Nt) ArrayFire arrays
+ * (Python/superloc/superloc.py).  All calls are asynchronous on `stream`. */
+
+/* PsfCorrMap2D (superloc.py:12-48): corr = conv(iq, conj(psf)) /
+ * sqrt(conv(|iq|^2, ones)) / psf_norm per frame, ArrayFire's same-size
+ * convolution (kernel element (kz/2, kx/2) on the output sample, zero
+ * outside the frame).  corr, iq: complex64 [nt][nx][nz]; psf: complex64
+ * [kx][kz] (column-major kz x kx); psf_norm = sqrt(sum |psf|^2) > 0;
+ * kz, kx <= 33 (RCABF_ERR_UNSUPPORTED beyond). */
+int rcabf_ulm_psf_corr(void *corr, const void *iq, const void *psf, float psf_norm, int64_t nz, int64_t nx,
+                       int64_t nt, int32_t kz, int32_t kx, void *stream);
+
+/* The ensemble map of SuperLocFilter (superloc.py:114-120): out(z, x, t) =
+ * sqrt|sum_f ker(f) p(t + nker/2 - f)| with p(u) = map(u) conj(map(u + 1)),
+ * t < nt - 1.  out: float [nt - 1][nx][nz]; map: complex64 [nt][nx][nz];
+ * ker: device float [nker] (the normalised Hann window). */
+int rcabf_ulm_ensemble(float *out, const void *map, const float *ker, int32_t nker, int64_t nz, int64_t nx,
+                       int64_t nt, void *stream);
+
+/* ImRegionalMax(I, 3) (superloc.py:51-53): bw = (3 x 3 dilation of map ==
+ * map) per frame; bw: uint8 [nt][nx][nz]; map: float [nt][nx][nz]. */
+int rcabf_ulm_regional_max(uint8_t *bw, const float *map, int64_t nz, int64_t nx, int64_t nt, void *stream);
+
+/* Candidate pixels of SuperLocFilter (superloc.py:51-53, 122-136) on the
+ * ensemble maps (float [nt][nx][nz], nt = their frame count): fit 0:
+ * regional maximum (3 x 3) of corr_ens with a regional maximum of env_ens
+ * within 3 x 3; fit 1: regional maximum of env_ens; z and x inside
+ * [edge, n - edge).  Writes, in no particular order, the column-major
+ * linear index and |value| of the fitted map (corr_ens for fit 0, env_ens
+ * for fit 1) of the first `capacity` candidates to lin / val, and the total
+ * candidate count to *count (device uint64). */
+int rcabf_ulm_detect(int64_t *lin, float *val, uint64_t *count, const float *corr_ens, const float *env_ens,
+                     int64_t nz, int64_t nx, int64_t nt, int32_t edge, int32_t fit, int64_t capacity, void *stream);
+
+/* Sub-pixel positions of n detections (superloc.py:56-100, 140-213): for
+ * each, the Hann-weighted least-squares parabola of log|map| over the
+ * (2 edge + 1)^2 neighbourhood, along x and z.  The detection's (x, z,
+ * frame) are read as the reference reads them, from a Fortran-flattened
+ * meshgrid at the linear index L: x = (L mod nz nx) div nx, z = L mod nx,
+ * frame = L div nz nx ((x, z) for square maps).  pos: device float [5][n]
+ * = (x + sub-x, 0, z + sub-z, val, frame); map: float [nt][nx][nz] (the
+ * fitted ensemble map); consts: device float, hann [(2e+1)^2] (z fastest),
+ * roi [2e+1], the row-major inverses of the x and z moment matrices [9],
+ * [9]. */
+int rcabf_ulm_gauss_fit(float *pos, const int64_t *lin, const float *val, int64_t n, const float *map, int64_t nz,
+                        int64_t nx, int64_t nt, int32_t edge, const float *consts, void *stream);
+
+/* Bins of DensityMappingND / VelocityMappingND(t) (superloc.py:216-402):
+ * per axis x, y, z, t the lowest bin edge, the mean bin step and the bin
+ * count; positions have pos_rows values each (x, y, z, value, frame),
+ * velocities vel_rows. */
+typedef struct rcabf_ulm_bins {
+    int32_t struct_size;   /* sizeof(rcabf_ulm_bins) */
+    int32_t pos_rows;
+    int32_t vel_rows;
+    int32_t reserved;
+    double min[4];
+    double step[4];
+    int64_t n[4];
+} rcabf_ulm_bins;
+
+/* Histograms of n positions (device double [n][pos_rows]): dens[z][x][y][t]
+ * += 1 and, when vel is not NULL, vel[c][z][x][y][t] += vel_in[i][c]
+ * (device double, zeroed by the caller).  A position's bin follows the
+ * reference: (p - min) / step cast to int16 as numpy does on x86-64,
+ * negatives to 0, indices past the last bin to the last bin and an index
+ * equal to the bin count to 0.  use_t = 0: no time axis (t extent 1). */
+int rcabf_ulm_density(double *dens, double *vel, const double *pos, int64_t n, const double *vel_in,
+                      const rcabf_ulm_bins *bins, int32_t use_t, void *stream);
+
 /* Count of device-side bound-check trips since the last call (expected 0). */
 int rcabf_take_error_count(int64_t *count);
 

@@ -97,6 +97,13 @@ class ServerStats(C.Structure):
     ]
 
 
+class UlmBins(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32), ("pos_rows", C.c_int32), ("vel_rows", C.c_int32), ("reserved", C.c_int32),
+        ("min", C.c_double * 4), ("step", C.c_double * 4), ("n", C.c_int64 * 4),
+    ]
+
+
 # Every symbol include/rcabf.h declares, with its ctypes signature.
 _SIGS = {
     "rcabf_status_string": (C.c_char_p, [C.c_int]),
@@ -123,6 +130,17 @@ _SIGS = {
     "rcabf_sim_element_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                           C.c_float, C.c_int, C.c_float, C.c_float, C.c_int64, C.c_int64,
                                           C.c_int64, C.c_int64, C.c_void_p]),
+    "rcabf_ulm_psf_corr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int64, C.c_int64,
+                                     C.c_int64, C.c_int32, C.c_int32, C.c_void_p]),
+    "rcabf_ulm_ensemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int64,
+                                     C.c_int64, C.c_void_p]),
+    "rcabf_ulm_regional_max": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_void_p]),
+    "rcabf_ulm_detect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                   C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int64, C.c_void_p]),
+    "rcabf_ulm_gauss_fit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                      C.c_int64, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
+    "rcabf_ulm_density": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                    C.POINTER(UlmBins), C.c_int32, C.c_void_p]),
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_measure_fp32_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),

@@ -44,7 +44,7 @@ def test_struct_layouts_match_header(tmp_path):
     src = tmp_path / "sz.c"
     structs = {"g": (L.GeometryDesc, "rcabf_geometry_desc"), "b": (L.BeamformArgs, "rcabf_beamform_args"),
                "c": (L.ServerConfig, "rcabf_server_config"), "s": (L.ServerStats, "rcabf_server_stats"),
-               "t": (L.TuneResult, "rcabf_tune_result")}
+               "t": (L.TuneResult, "rcabf_tune_result"), "u": (L.UlmBins, "rcabf_ulm_bins")}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rcabf.h"', "int main(void){"]
     for tag, (py, cname) in structs.items():
         lines.append(f'printf("{tag} %zu\\n", sizeof({cname}));')
@@ -88,3 +88,23 @@ def test_server_argument_checks_need_no_device():
     assert lib.rcabf_server_poll(None, 1, C.byref(st)) == 108
     assert lib.rcabf_server_wait_for(None, 1, 0.0, C.byref(st)) == 108
     assert lib.rcabf_server_destroy(None) == 108
+
+
+def test_ulm_argument_checks_need_no_device():
+    lib = L.lib()
+    assert lib.rcabf_ulm_psf_corr(None, None, None, 1.0, 8, 8, 2, 3, 3, None) == 100
+    assert lib.rcabf_ulm_ensemble(None, None, None, 5, 8, 8, 2, None) == 100
+    n = C.c_uint64()
+    assert lib.rcabf_ulm_detect(None, None, C.byref(n), None, None, 8, 8, 2, 3, 0, 0, None) == 100
+    assert lib.rcabf_ulm_gauss_fit(None, None, None, 1, None, 8, 8, 2, 3, None, None) == 100
+    b = L.UlmBins()
+    b.struct_size = 8                                          # wrong size
+    assert lib.rcabf_ulm_density(None, None, None, 0, None, C.byref(b), 0, None) == 100
+    b.struct_size = C.sizeof(L.UlmBins)
+    b.pos_rows = 5
+    for k in range(3):
+        b.n[k], b.step[k] = 4, 1.0
+    assert lib.rcabf_ulm_density(C.c_void_p(1), None, None, 0, None, C.byref(b), 0, None) == 0   # nothing to bin
+    b.step[1] = 0.0
+    assert lib.rcabf_ulm_density(C.c_void_p(1), None, None, 0, None, C.byref(b), 0, None) == 101
+
