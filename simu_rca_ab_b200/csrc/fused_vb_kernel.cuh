@@ -177,24 +177,44 @@ __device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&f
     }
 }
 
-// Weighted row sums of one frame pair for every voxel: ts[v] = sum_k
-// ws[v][k] * row k (re, im of frame 2p; re, im of frame 2p + 1).
+// Weighted row sums of one frame pair for every voxel: lo[v] = sum_k
+// ws[v][k] * (word 0, word 1) of row k, hi[v] = the same of (word 2, word
+// 3), two FP32 FMAs per instruction (fma.rn.f32x2, the same IEEE operation
+// on each half as fmaf).  Rows hold a frame pair as (re0, im0, re1, im1)
+// when staged by cp.async (complex64 slabs) and as (re0, re1, im0, im1)
+// when staged from registers (FP16/BF16 slabs): see VbPlanar.
 template <int R, int STRIDE>
-__device__ __forceinline__ void vb_pair_sums(const char *rows, const float (&ws)[VB][R], float4 (&ts)[VB])
+__device__ __forceinline__ void vb_pair_sums(const char *rows, const float (&ws)[VB][R], float2 (&lo)[VB],
+                                             float2 (&hi)[VB])
 {
 #pragma unroll
-    for (int v = 0; v < VB; ++v) ts[v] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int v = 0; v < VB; ++v) { lo[v] = make_float2(0.f, 0.f); hi[v] = make_float2(0.f, 0.f); }
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const float4 x = *reinterpret_cast<const float4 *>(rows + k * STRIDE);
+        const float2 xl = make_float2(x.x, x.y), xh = make_float2(x.z, x.w);
 #pragma unroll
         for (int v = 0; v < VB; ++v) {
-            ts[v].x = fmaf(ws[v][k], x.x, ts[v].x);
-            ts[v].y = fmaf(ws[v][k], x.y, ts[v].y);
-            ts[v].z = fmaf(ws[v][k], x.z, ts[v].z);
-            ts[v].w = fmaf(ws[v][k], x.w, ts[v].w);
+            const float2 w2 = make_float2(ws[v][k], ws[v][k]);
+            lo[v] = __ffma2_rn(w2, xl, lo[v]);
+            hi[v] = __ffma2_rn(w2, xh, hi[v]);
         }
     }
+}
+
+// Staged frame-pair layout: planar (re0, re1, im0, im1) for register
+// staging, where the conversion writes the words in any order, so that the
+// phasor products of both frames pair up (re with re, im with im) for
+// fma.rn.f32x2; interleaved (re0, im0, re1, im1) for cp.async staging,
+// which copies complex64 slabs as they are.
+template <int STORE> struct VbPlanar { static constexpr bool value = STORE != ST_F32; };
+
+// (re, im) of frames 2p, 2p + 1 from a pair's four words in the layout
+template <bool PL>
+__device__ __forceinline__ void vb_unpack(float w0, float w1, float w2, float w3, float2 &f0, float2 &f1)
+{
+    if constexpr (PL) { f0 = make_float2(w0, w2); f1 = make_float2(w1, w3); }
+    else { f0 = make_float2(w0, w1); f1 = make_float2(w2, w3); }
 }
 
 template <int KIND, int FB, int STORE, int D, bool TM>
@@ -208,6 +228,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
     constexpr int TAPS = KT::TAPS;
     constexpr int R = TAPS + D;                        // rows a thread reads per step
     constexpr bool ASYNC = (STORE == ST_F32);
+    constexpr bool PL = VbPlanar<STORE>::value;        // staged frame-pair layout
     constexpr int NST = ASYNC ? 3 : 2;
     constexpr int ES = (int)sizeof(T);
     constexpr int RAWB = FB * ES;
@@ -285,7 +306,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
 #pragma unroll
             for (int f = 0; f < FB; ++f) acc[v][f] = make_float2(0.f, 0.f);
         // TM: words [16 p, 16 p + 16) of a lane hold frames 2p, 2p + 1 of
-        // its voxels: voxel v at 4 v + {re 2p, im 2p, re 2p+1, im 2p+1}
+        // its voxels: voxel v at 4 v + the staged layout (VbPlanar: re 2p,
+        // re 2p+1, im 2p, im 2p+1; else re 2p, im 2p, re 2p+1, im 2p+1)
         auto tm_zero = [&]() {
             uint32_t z[16];
 #pragma unroll
@@ -307,10 +329,9 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     tmem_ld16(tlane + (uint32_t)(c * 8), w);
                     tmem_wait_ld16(w);
 #pragma unroll
-                    for (int v = 0; v < VB; ++v) {
-                        a[v][0] = make_float2(__uint_as_float(w[4 * v]), __uint_as_float(w[4 * v + 1]));
-                        a[v][1] = make_float2(__uint_as_float(w[4 * v + 2]), __uint_as_float(w[4 * v + 3]));
-                    }
+                    for (int v = 0; v < VB; ++v)
+                        vb_unpack<PL>(__uint_as_float(w[4 * v]), __uint_as_float(w[4 * v + 1]),
+                                      __uint_as_float(w[4 * v + 2]), __uint_as_float(w[4 * v + 3]), a[v][0], a[v][1]);
                 } else {
 #pragma unroll
                     for (int v = 0; v < VB; ++v) { a[v][0] = acc[v][c]; a[v][1] = acc[v][c + 1]; }
@@ -395,7 +416,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     for (int v = 0; v < CS / 4; v += 2) {
                         if (v + 1 < CS / 4) {
                             const float2 x0 = packed16_to_f2(b[v], STORE), x1 = packed16_to_f2(b[v + 1], STORE);
-                            *reinterpret_cast<float4 *>(o + v) = make_float4(x0.x, x0.y, x1.x, x1.y);
+                            // planar frame pair (re0, re1, im0, im1), VbPlanar
+                            *reinterpret_cast<float4 *>(o + v) = make_float4(x0.x, x1.x, x0.y, x1.y);
                         } else {
                             o[v] = packed16_to_f2(b[v], STORE);
                         }
@@ -482,15 +504,17 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                                                (s % NST) * stage_bytes + row0 * STRIDE;
 #pragma unroll
                             for (int c = 0; c < FB; c += 2) {
-                                float4 ts[VB];
-                                vb_pair_sums<R, STRIDE>(rows + c * 8, ws, ts);
+                                float2 lo[VB], hi[VB];
+                                vb_pair_sums<R, STRIDE>(rows + c * 8, ws, lo, hi);
 #pragma unroll
                                 for (int v = 0; v < VB; ++v) {
+                                    float2 t0, t1;   // interpolated (re, im) of frames c, c + 1
+                                    vb_unpack<PL>(lo[v].x, lo[v].y, hi[v].x, hi[v].y, t0, t1);
                                     float2 &a0 = acc[v][c], &a1 = acc[v][c + 1];
-                                    a0.x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0.x));
-                                    a0.y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0.y));
-                                    a1.x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1.x));
-                                    a1.y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1.y));
+                                    a0.x = fmaf(P[v].x, t0.x, fmaf(-P[v].y, t0.y, a0.x));
+                                    a0.y = fmaf(P[v].x, t0.y, fmaf(P[v].y, t0.x, a0.y));
+                                    a1.x = fmaf(P[v].x, t1.x, fmaf(-P[v].y, t1.y, a1.x));
+                                    a1.y = fmaf(P[v].x, t1.y, fmaf(P[v].y, t1.x, a1.y));
                                 }
                             }
                         }
@@ -539,21 +563,35 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     for (int c = 0; c < FB; c += 2) {
                         uint32_t w[16];
                         tmem_ld16(tlane + (uint32_t)(c * 8), w);
-                        float4 ts[VB];
-                        vb_pair_sums<R, STRIDE>(rows + c * 8, ws, ts);
+                        float2 lo[VB], hi[VB];
+                        vb_pair_sums<R, STRIDE>(rows + c * 8, ws, lo, hi);
                         tmem_wait_ld16(w);
 #pragma unroll
                         for (int v = 0; v < VB; ++v) {
-                            const float a0x = __uint_as_float(w[4 * v]), a0y = __uint_as_float(w[4 * v + 1]);
-                            const float a1x = __uint_as_float(w[4 * v + 2]), a1y = __uint_as_float(w[4 * v + 3]);
-                            const float n0x = fmaf(P[v].x, ts[v].x, fmaf(-P[v].y, ts[v].y, a0x));
-                            const float n0y = fmaf(P[v].x, ts[v].y, fmaf(P[v].y, ts[v].x, a0y));
-                            const float n1x = fmaf(P[v].x, ts[v].z, fmaf(-P[v].y, ts[v].w, a1x));
-                            const float n1y = fmaf(P[v].x, ts[v].w, fmaf(P[v].y, ts[v].z, a1y));
-                            w[4 * v] = __float_as_uint(n0x);
-                            w[4 * v + 1] = __float_as_uint(n0y);
-                            w[4 * v + 2] = __float_as_uint(n1x);
-                            w[4 * v + 3] = __float_as_uint(n1y);
+                            if constexpr (PL) {
+                                // words (re0, re1, im0, im1); lo = interpolated re of
+                                // both frames, hi = im: re += Px re - Py im, im +=
+                                // Px im + Py re, both frames per fma.rn.f32x2, in
+                                // the scalar kernel's order
+                                float2 re = make_float2(__uint_as_float(w[4 * v]), __uint_as_float(w[4 * v + 1]));
+                                float2 im = make_float2(__uint_as_float(w[4 * v + 2]), __uint_as_float(w[4 * v + 3]));
+                                const float2 px = make_float2(P[v].x, P[v].x), py = make_float2(P[v].y, P[v].y);
+                                const float2 npy = make_float2(-P[v].y, -P[v].y);
+                                re = __ffma2_rn(px, lo[v], __ffma2_rn(npy, hi[v], re));
+                                im = __ffma2_rn(px, hi[v], __ffma2_rn(py, lo[v], im));
+                                w[4 * v] = __float_as_uint(re.x);
+                                w[4 * v + 1] = __float_as_uint(re.y);
+                                w[4 * v + 2] = __float_as_uint(im.x);
+                                w[4 * v + 3] = __float_as_uint(im.y);
+                            } else {
+                                const float a0x = __uint_as_float(w[4 * v]), a0y = __uint_as_float(w[4 * v + 1]);
+                                const float a1x = __uint_as_float(w[4 * v + 2]), a1y = __uint_as_float(w[4 * v + 3]);
+                                const float2 t0 = lo[v], t1 = hi[v];
+                                w[4 * v] = __float_as_uint(fmaf(P[v].x, t0.x, fmaf(-P[v].y, t0.y, a0x)));
+                                w[4 * v + 1] = __float_as_uint(fmaf(P[v].x, t0.y, fmaf(P[v].y, t0.x, a0y)));
+                                w[4 * v + 2] = __float_as_uint(fmaf(P[v].x, t1.x, fmaf(-P[v].y, t1.y, a1x)));
+                                w[4 * v + 3] = __float_as_uint(fmaf(P[v].x, t1.y, fmaf(P[v].y, t1.x, a1y)));
+                            }
                         }
                         tmem_st16(tlane + (uint32_t)(c * 8), w);
                     }
