@@ -556,10 +556,10 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                                        (use ? (s % NST) * stage_bytes + row0 * STRIDE : zero_off);
                     __syncwarp();     // converged after the divergent checks above
                     tmem_wait_st();   // the previous step's stores are visible to the loads below
-                    // (two pairs per iteration: fully unrolled, the loop spills at
-                    // 128 registers and measured 14% slower; one pair per
-                    // iteration measured 1.4% slower than two)
-#pragma unroll 2
+                    // (one pair per iteration: unrolled by two the loop spills 56
+                    // bytes at 128 registers and measured 0.6% slower, fully
+                    // unrolled it measured 14% slower)
+#pragma unroll 1
                     for (int c = 0; c < FB; c += 2) {
                         uint32_t w[16];
                         tmem_ld16(tlane + (uint32_t)(c * 8), w);
