@@ -14,9 +14,10 @@ tables, the fused delay-and-sum kernel over all frames and transmits, and
 the mask.
 
 value     : device-resident inputs, CUDA events on the launching stream.
-e2e       : the same through the C ABI with host (pinned) buffers: the
-            step's H2D copy of the channel data and D2H copy of the volume
-            are inside the timed region.
+e2e       : the same through the C ABI with host (pinned) buffers
+            (rcabf_beamform_host): the step's H2D copy of the channel data
+            and D2H copy of the volume are inside the timed region, in frame
+            chunks overlapped with the beamforming.
 roofline  : the fused kernel's FP32 work (active units x (8a + 8) FLOP)
             over its event-timed duration, against the FP32 FMA peak measured
             live on this GPU.
@@ -583,19 +584,25 @@ def main():
                 "ranges": sum(ee[1].elapsed_time(ee[2]) for ee in evs),
                 "das": fused_ms, "mask": sum(ee[3].elapsed_time(ee[4]) for ee in evs)}
 
-    # e2e: host pinned buffers through the C ABI
+    # e2e: host pinned buffers through the C ABI (rcabf_beamform_host: the
+    # frames go through in chunks, each chunk's copies in and out overlapping
+    # the beamforming of its neighbours)
     e2e = None
     if not a.no_e2e:
         host_in = [t.cpu().pin_memory() for t in iq_dev]
         host_out = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
-        h2d = sum(t.numel() * t.element_size() for t in host_in)
-        d2h = host_out.numel() * host_out.element_size()
+        out_bytes = host_out.numel() * host_out.element_size()
+        # later groups add into the output: their chunks are read in as well
+        h2d = sum(t.numel() * t.element_size() for t in host_in) + out_bytes * (len(geoms) - 1)
+        d2h = out_bytes * len(geoms)
+        host_args = [eng.make_args(g, host_in[gi], iq_dtype=iq_code, n_sample=w.n_sample, n_frame=F, out=host_out,
+                                   mask=mask, compound=True, storage=st_code, kernel=kern, accumulate=gi > 0,
+                                   frames_per_block=a.frames_per_block, host=True)
+                     for gi, g in enumerate(geoms)]
 
         def e2e_step():
-            for t_h, t_d in zip(host_in, iq_dev):
-                t_d.copy_(t_h, non_blocking=True)
-            step()
-            host_out.copy_(out, non_blocking=True)
+            for g, ar in zip(geoms, host_args):
+                eng.run_host(g, ar, 0, stream)
 
         for _ in range(2):
             e2e_step()

@@ -244,6 +244,28 @@ int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *
 int rcabf_beamform_batch(int n, const rcabf_geometry *const *g, const rcabf_beamform_args *a,
                          void *stream);
 
+/* rcabf_beamform with the channel data (a->iq) and the output (a->out) in
+ * HOST memory, page-locked for the copies to overlap (cudaHostAlloc /
+ * cudaHostRegister): the frames go through in chunks of frames_per_chunk
+ * (0: about four chunks of whole frame blocks, the last the shortest), each
+ * chunk copied in on a copy stream, beamformed on `stream` and copied out on
+ * another, so that the copies of one chunk overlap the beamforming of its
+ * neighbours and only the first copy in and the last copy out are exposed.
+ * Same results as rcabf_beamform on device copies of the buffers.
+ * a->workspace: device scratch of rcabf_beamform_host_workspace_size bytes
+ * (two chunks of channel data and of output, and one chunk's beamform
+ * workspace); a->mask stays a device pointer (computed with the first
+ * chunk); accumulate = 1 reads each output chunk in before adding to it;
+ * per_channel output is RCABF_ERR_UNSUPPORTED (not frame-major).
+ * Asynchronous on `stream`: the output is in host memory, and the host
+ * buffers free, once `stream` reaches this call.  Replaces the reference's
+ * per-chunk host/device round trip (bfVirtualSourceGeneric_RCA.m:664-711:
+ * gpuArray upload, feval, gather), which serialises copies and kernels. */
+int rcabf_beamform_host_workspace_size(const rcabf_geometry *g, const rcabf_beamform_args *a,
+                                       int32_t frames_per_chunk, size_t *bytes);
+int rcabf_beamform_host(const rcabf_geometry *g, const rcabf_beamform_args *a, int32_t frames_per_chunk,
+                        void *stream);
+
 /* Size of the static device workspace of rcabf_beamform_noalloc (64 MiB). */
 #define RCABF_NOALLOC_WORKSPACE_BYTES ((size_t)64 << 20)
 

@@ -119,6 +119,9 @@ _SIGS = {
     "rcabf_describe_plan": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_char_p, C.c_size_t]),
     "rcabf_beamform_batch": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(BeamformArgs), C.c_void_p]),
     "rcabf_beamform_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p]),
+    "rcabf_beamform_host_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_int32,
+                                                     C.POINTER(C.c_size_t)]),
+    "rcabf_beamform_host": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_int32, C.c_void_p]),
     "rcabf_autotune": (C.c_int, [C.c_void_p, C.POINTER(BeamformArgs), C.c_void_p, C.c_int,
                                  C.POINTER(TuneResult)]),
     "rcabf_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),

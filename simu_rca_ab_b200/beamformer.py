@@ -176,9 +176,10 @@ class Engine:
     def make_args(self, geom: GeometryHandle, iq: "torch.Tensor", *, iq_dtype: int, n_sample: int,
                   n_frame: int, out: "torch.Tensor", mask: "torch.Tensor | None", compound: bool,
                   storage: int = L.STORE_F32, kernel: int = L.KERNEL_AUTO, accumulate: bool = False,
-                  frames_per_block: int = 0, per_channel: bool = False) -> L.BeamformArgs:
+                  frames_per_block: int = 0, per_channel: bool = False, host: bool = False) -> L.BeamformArgs:
         # The C ABI takes raw pointers: check every buffer holds what the
-        # sizes claim before handing it over.
+        # sizes claim before handing it over.  host: iq and out in host
+        # memory (pinned for overlap) for run_host; the mask stays on the device.
         T = 1 if compound else geom.n_tx
         dt, per_sample = _IQ_TORCH[iq_dtype]
         if iq.dtype != dt:
@@ -194,9 +195,11 @@ class Engine:
             raise ValueError("out must be a contiguous complex64 tensor of ([element] x) frames x (1 or tx) x pixels")
         if mask is not None and (mask.dtype != torch.float32 or mask.numel() < T * geom.n_pix):
             raise ValueError("mask must be a float32 tensor of (1 or tx) x pixels")
-        for t in (iq, out) + ((mask,) if mask is not None else ()):
+        for t in ((mask,) if mask is not None else ()) + (() if host else (iq, out)):
             if t.device != self.device:
                 raise ValueError(f"tensor on {t.device}, engine on {self.device}")
+        if host and (iq.device.type != "cpu" or out.device.type != "cpu"):
+            raise ValueError("host=True: channel data and output must be host tensors (pinned for overlap)")
         a = L.BeamformArgs()
         a.struct_size = C.sizeof(L.BeamformArgs)
         a.iq_dtype = iq_dtype
@@ -252,6 +255,23 @@ class Engine:
         a.workspace_bytes = ws.numel() if need else 0
         with torch.cuda.device(self.device):
             L.check(L.lib().rcabf_beamform(C.c_void_p(geom.ptr), C.byref(a), C.c_void_p(sp)), "rcabf_beamform")
+
+    def run_host(self, geom: GeometryHandle, a: L.BeamformArgs, frames_per_chunk: int = 0, stream=None,
+                 workspace=None) -> None:
+        """rcabf_beamform_host: channel data and output in host memory (args
+        made with host=True), frames in chunks whose copies in and out
+        overlap the beamforming of their neighbours.  Asynchronous on
+        `stream`: synchronise it before reading the output."""
+        sp = _stream_ptr(stream)
+        n = C.c_size_t()
+        L.check(L.lib().rcabf_beamform_host_workspace_size(C.c_void_p(geom.ptr), C.byref(a), frames_per_chunk,
+                                                           C.byref(n)), "rcabf_beamform_host_workspace_size")
+        ws = workspace if workspace is not None else self._workspace(n.value, sp)
+        a.workspace = ws.data_ptr()
+        a.workspace_bytes = ws.numel()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().rcabf_beamform_host(C.c_void_p(geom.ptr), C.byref(a), frames_per_chunk, C.c_void_p(sp)),
+                    "rcabf_beamform_host")
 
     def run_batch(self, geoms: list, args: list, workspaces: list, stream=None) -> None:
         """One persistent fused launch over several acquisitions."""

@@ -605,6 +605,167 @@ int rcabf_beamform(const rcabf_geometry *g, const rcabf_beamform_args *a, void *
     return beamform_one(const_cast<rcabf_geometry *>(g), a, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------------------------------------
+// Host-buffer beamforming: frames in chunks, copies overlapped with compute
+// ---------------------------------------------------------------------------
+namespace {
+
+size_t iq_sample_bytes(int iq_dtype) { return iq_dtype == RCABF_IQ_C64 ? 8 : iq_dtype == RCABF_IQ_RF_F32 ? 8 : 4; }
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Chunk length (whole frame blocks of the full call's plan, the last chunk
+// the shortest) and the device buffers of two chunks in the workspace.
+struct HostLayout {
+    int64_t chunk = 0;
+    size_t in_bytes = 0, out_bytes = 0, plan_bytes = 0, total = 0;
+    bool have_tuned = false;   // the autotuner's choice for the whole call, used by every chunk
+    TuneChoice tuned;
+};
+
+// Plan of one chunk: the whole call's tuned choice where one exists and fits.
+int chunk_plan(rcabf_geometry *g, const rcabf_beamform_args *c, const HostLayout &h, Plan &p)
+{
+    if (h.have_tuned && plan_beamform(g, c, p, &h.tuned) == RCABF_OK) return RCABF_OK;
+    return plan_beamform(g, c, p);
+}
+
+int host_layout(rcabf_geometry *g, const rcabf_beamform_args *a, int32_t frames_per_chunk, HostLayout &h)
+{
+    if (a->per_channel) return RCABF_ERR_UNSUPPORTED;   // [element][frame]... output: not frame-major
+    if (frames_per_chunk < 0) return RCABF_ERR_INVALID_ARGUMENT;
+    Plan p;
+    int s = plan_beamform(g, a, p);
+    if (s != RCABF_OK) return s;
+    int64_t chunk = frames_per_chunk;
+    if (chunk == 0) {
+        // about four chunks of whole frame blocks: the first copy in and the
+        // last copy out are the only transfers not hidden under compute
+        const int64_t fb = p.kernel == RCABF_KERNEL_FUSED ? p.fb : 1;
+        const int64_t n_fb = (a->n_frame + fb - 1) / fb;
+        chunk = fb * ((n_fb + 3) / 4);
+    }
+    h.chunk = std::min<int64_t>(chunk, a->n_frame);
+    {
+        std::lock_guard<std::mutex> lk(g->mu);
+        auto it = g->tuned.find({a->n_frame, (int64_t)a->storage});
+        if (it != g->tuned.end() && p.kernel == RCABF_KERNEL_FUSED && it->second.fb == p.fb && it->second.vb == p.vb) {
+            h.have_tuned = true;
+            h.tuned = it->second;
+        }
+    }
+    const int64_t n_t = a->compound ? 1 : a->n_tx;
+    h.in_bytes = align256((size_t)h.chunk * a->n_tx * a->n_ch * a->n_sample * iq_sample_bytes(a->iq_dtype));
+    h.out_bytes = align256((size_t)h.chunk * n_t * g->n_pix * 8);
+    rcabf_beamform_args c = *a;
+    c.n_frame = h.chunk;
+    Plan pc;
+    if ((s = chunk_plan(g, &c, h, pc)) != RCABF_OK) return s;
+    h.plan_bytes = align256(pc.total);
+    h.total = 2 * h.in_bytes + 2 * h.out_bytes + h.plan_bytes;
+    return RCABF_OK;
+}
+
+}  // namespace
+
+int rcabf_beamform_host_workspace_size(const rcabf_geometry *g, const rcabf_beamform_args *a,
+                                       int32_t frames_per_chunk, size_t *bytes)
+{
+    if (!g) return RCABF_ERR_BAD_HANDLE;
+    if (!a || !bytes) return RCABF_ERR_INVALID_ARGUMENT;
+    HostLayout h;
+    const int s = host_layout(const_cast<rcabf_geometry *>(g), a, frames_per_chunk, h);
+    if (s == RCABF_OK) *bytes = h.total;
+    return s;
+}
+
+int rcabf_beamform_host(const rcabf_geometry *g0, const rcabf_beamform_args *a, int32_t frames_per_chunk,
+                        void *stream)
+{
+    if (!g0) return RCABF_ERR_BAD_HANDLE;
+    if (!a || !a->iq || !a->out) return RCABF_ERR_INVALID_ARGUMENT;
+    rcabf_geometry *g = const_cast<rcabf_geometry *>(g0);
+    HostLayout h;
+    int s = host_layout(g, a, frames_per_chunk, h);
+    if (s != RCABF_OK) return s;
+    if (a->workspace_bytes < h.total || !a->workspace) return RCABF_ERR_WORKSPACE_TOO_SMALL;
+    if (((uintptr_t)a->workspace) % 256) return RCABF_ERR_INVALID_ARGUMENT;
+    char *ws = static_cast<char *>(a->workspace);
+    char *dev_in[2] = {ws, ws + h.in_bytes};
+    char *dev_out[2] = {ws + 2 * h.in_bytes, ws + 2 * h.in_bytes + h.out_bytes};
+    char *plan_ws = ws + 2 * h.in_bytes + 2 * h.out_bytes;
+    const cudaStream_t st = (cudaStream_t)stream;
+    const size_t in_frame = (size_t)a->n_tx * a->n_ch * a->n_sample * iq_sample_bytes(a->iq_dtype);
+    const size_t out_frame = (size_t)(a->compound ? 1 : a->n_tx) * g->n_pix * 8;
+
+    // copy-in and copy-out streams; events order the three per buffer slot
+    cudaStream_t cin = nullptr, cout = nullptr;
+    cudaEvent_t ev[7] = {};   // start, in_ready[2], done[2], out_done[2]
+    auto cleanup = [&]() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);   // released once pending work that uses it completes
+        if (cin) cudaStreamDestroy(cin);
+        if (cout) cudaStreamDestroy(cout);
+    };
+    cudaError_t ce = cudaStreamCreateWithFlags(&cin, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&cout, cudaStreamNonBlocking);
+    for (int i = 0; i < 7 && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    if (ce != cudaSuccess) { cleanup(); return cuda_fail(ce, "host pipeline streams"); }
+    cudaEvent_t start = ev[0], *in_ready = ev + 1, *done = ev + 3, *out_done = ev + 5;
+    // the copies follow the caller's earlier work on `stream`
+    ce = cudaEventRecord(start, st);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cin, start, 0);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cout, start, 0);
+
+    const char *host_in = static_cast<const char *>(a->iq);
+    char *host_out = static_cast<char *>(a->out);
+    for (int64_t f0 = 0, c = 0; f0 < a->n_frame && ce == cudaSuccess && s == RCABF_OK; f0 += h.chunk, ++c) {
+        const int b = (int)(c % 2);
+        const int64_t nf = std::min<int64_t>(h.chunk, a->n_frame - f0);
+        // in: slot b is free once chunk c - 2 is computed (and copied out,
+        // when the output chunk is loaded for accumulation)
+        if (c >= 2) ce = cudaStreamWaitEvent(cin, done[b], 0);
+        if (ce == cudaSuccess && c >= 2 && a->accumulate) ce = cudaStreamWaitEvent(cin, out_done[b], 0);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(dev_in[b], host_in + f0 * in_frame, nf * in_frame, cudaMemcpyHostToDevice, cin);
+        if (ce == cudaSuccess && a->accumulate)
+            ce = cudaMemcpyAsync(dev_out[b], host_out + f0 * out_frame, nf * out_frame, cudaMemcpyHostToDevice, cin);
+        if (ce == cudaSuccess) ce = cudaEventRecord(in_ready[b], cin);
+        // compute on the caller's stream, into slot b once its last copy-out ended
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, in_ready[b], 0);
+        if (ce == cudaSuccess && c >= 2 && !a->accumulate) ce = cudaStreamWaitEvent(st, out_done[b], 0);
+        if (ce != cudaSuccess) break;
+        rcabf_beamform_args ca = *a;
+        ca.iq = dev_in[b];
+        ca.out = dev_out[b];
+        ca.n_frame = nf;
+        ca.mask = c == 0 ? a->mask : nullptr;   // the mask does not depend on frames: once
+        ca.workspace = plan_ws;
+        ca.workspace_bytes = h.plan_bytes;
+        ca.stage_events = nullptr;
+        Plan pc;
+        s = chunk_plan(g, &ca, h, pc);
+        if (s == RCABF_OK) s = beamform_planned(g, &ca, pc, st);
+        if (s != RCABF_OK) break;
+        ce = cudaEventRecord(done[b], st);
+        // out
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cout, done[b], 0);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(host_out + f0 * out_frame, dev_out[b], nf * out_frame, cudaMemcpyDeviceToHost, cout);
+        if (ce == cudaSuccess) ce = cudaEventRecord(out_done[b], cout);
+    }
+    // the caller's stream completes after the last copies out
+    if (ce == cudaSuccess) ce = cudaEventRecord(out_done[0], cout);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, out_done[0], 0);
+    if (ce != cudaSuccess || s != RCABF_OK) {
+        // no copy may still touch the caller's host buffers after an error return
+        cudaStreamSynchronize(cin);
+        cudaStreamSynchronize(cout);
+    }
+    cleanup();
+    if (ce != cudaSuccess) return cuda_fail(ce, "host pipeline");
+    return s;
+}
+
 int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream)
 {
     if (!g) return RCABF_ERR_BAD_HANDLE;

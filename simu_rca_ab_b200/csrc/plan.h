@@ -14,7 +14,7 @@ constexpr size_t SMEM_BUDGET = 110 * 1024;
 
 struct Plan {
     int kernel = 0;       // rcabf_kernel
-    int vb = 0;           // 1: voxel-blocked kernel (fused_vb_kernel.cuh)
+    int vb = 0;           // voxel-blocked kernel (fused_vb_kernel.cuh): 1 register, 2 TMEM accumulators
     int d = 0;            // its row shift bound
     int store = 0;
     int fb = 1, n_fb = 1;

@@ -90,6 +90,13 @@ def test_server_argument_checks_need_no_device():
     assert lib.rcabf_server_destroy(None) == 108
 
 
+def test_host_pipeline_argument_checks_need_no_device():
+    lib = L.lib()
+    n = C.c_size_t()
+    assert lib.rcabf_beamform_host_workspace_size(None, None, 0, C.byref(n)) == 108
+    assert lib.rcabf_beamform_host(None, None, 0, None) == 108
+
+
 def test_ulm_argument_checks_need_no_device():
     lib = L.lib()
     assert lib.rcabf_ulm_psf_corr(None, None, None, 1.0, 8, 8, 2, 3, 3, None) == 100
