@@ -203,7 +203,12 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
                     if (tm && c < 8) continue;
                     if (force && c != force->fb) continue;
                     if (!force && fb_req > 0 && c != fb_req) continue;
-                    if (!force && fb_req == 0 && c > 2 * a->n_frame) continue;
+                    // the planner's choice: at most the frame count rounded up to a
+                    // power of two (a block more than half empty costs more than
+                    // the setup it saves: per item t ~ setup + FB x frame cost,
+                    // setup ~ 13 frames); a store asked for by name may pad to 2x
+                    const int64_t lim = want_vb ? 2 * a->n_frame : pow2_ceil(a->n_frame);
+                    if (!force && fb_req == 0 && c > lim) continue;
                     const int cap = std::min<int>((int)(VB_SMEM_BUDGET / ((size_t)fused_stages(p.store) *
                                                                            fused_row_words(c) * 4)),
                                                   vb_stage_rows_cap(p.store, c));
@@ -903,9 +908,9 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
                 if (fb == p0.fb || fb > 2 * a->n_frame) continue;
                 consider(TuneChoice{p0.vb, fb, bt});
             }
-            // the other accumulator store (registers / tensor memory) at the
-            // frame blocks tensor memory takes
-            for (int fb : {8, 16}) {
+            // the other accumulator store (registers / tensor memory) at every
+            // frame block it takes (tensor memory: 8 and 16)
+            for (int fb : {2, 4, 8, 16}) {
                 if (fb > 2 * a->n_frame) continue;
                 consider(TuneChoice{p0.vb == 2 ? 1 : 2, fb, bt});
             }
