@@ -122,7 +122,7 @@ typedef enum rcabf_kernel {
     RCABF_KERNEL_FUSED_NOBLOCK = 3, /* the fused kernel with one voxel per thread */
     /* the voxel-blocked fused kernel with a given accumulator store
        (RCABF_ERR_UNSUPPORTED where the geometry allows no voxel blocking):
-       tensor memory (frame blocks of 8 or 16; sm_100a TMEM) or registers */
+       tensor memory (sm_100a TMEM) or registers */
     RCABF_KERNEL_FUSED_TMEM = 4,
     RCABF_KERNEL_FUSED_REGS = 5
 } rcabf_kernel;

@@ -200,7 +200,6 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
                 g->window_rows(TileShape{vts.tu, vts.tv * VB_BLOCK, vts.tz}) + d, a->n_sample);
             auto pick_fb = [&](int tm) {   // the largest frame block whose window fits
                 for (int c : {16, 8, 4, 2}) {
-                    if (tm && c < 8) continue;
                     if (force && c != force->fb) continue;
                     if (!force && fb_req > 0 && c != fb_req) continue;
                     // the planner's choice: at most the frame count rounded up to a
@@ -909,7 +908,7 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
                 consider(TuneChoice{p0.vb, fb, bt});
             }
             // the other accumulator store (registers / tensor memory) at every
-            // frame block it takes (tensor memory: 8 and 16)
+            // frame block
             for (int fb : {2, 4, 8, 16}) {
                 if (fb > 2 * a->n_frame) continue;
                 consider(TuneChoice{p0.vb == 2 ? 1 : 2, fb, bt});

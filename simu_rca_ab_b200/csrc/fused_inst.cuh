@@ -135,14 +135,15 @@ static cudaError_t vb_do(const FusedParams *p, int grid, size_t smem, cudaStream
     return cudaGetLastError();
 }
 
-// tm: accumulators in tensor memory (frame blocks of 8 and 16 only, where
-// they take 64 / 128 registers otherwise)
+// tm: accumulators in tensor memory (32 to 128 columns per CTA)
 template <int KIND, int STORE, int D>
 static cudaError_t vb_fb(int tm, int fb, const FusedParams *p, int grid, size_t smem, cudaStream_t st, int what,
                          int *occ)
 {
     if (tm) {
         switch (fb) {
+        case 2: return vb_do<KIND, 2, STORE, D, true>(p, grid, smem, st, what, occ);
+        case 4: return vb_do<KIND, 4, STORE, D, true>(p, grid, smem, st, what, occ);
         case 8: return vb_do<KIND, 8, STORE, D, true>(p, grid, smem, st, what, occ);
         case 16: return vb_do<KIND, 16, STORE, D, true>(p, grid, smem, st, what, occ);
         default: return cudaErrorInvalidValue;

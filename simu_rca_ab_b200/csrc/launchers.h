@@ -63,7 +63,7 @@ int fused_occupancy(int mode, int kind, int fb, int store, size_t smem);
 
 // Voxel-blocked fused kernel (EXACT tables): d = row shift bound (1 or 2),
 // fb in {2, 4, 8, 16}; 128 threads per CTA; tm = 1: accumulators in tensor
-// memory (fb 8 and 16), occupancy capped by the SM's 512 TMEM columns.
+// memory, occupancy capped by the SM's 512 TMEM columns.
 cudaError_t launch_fused_vb(int kind, int d, int tm, int fb, int store, const FusedParams &p, int grid,
                             size_t smem, cudaStream_t st);
 cudaError_t prepare_fused_vb(int kind, int d, int tm, int fb, int store, size_t smem);

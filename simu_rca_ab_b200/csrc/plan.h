@@ -47,8 +47,8 @@ inline size_t fused_smem_bytes(int mode, int kind, int store, int wmax, int row_
 }
 // The voxel-blocked kernel keeps no table; three CTAs of 128 threads share an SM.
 constexpr size_t VB_SMEM_BUDGET = 72 * 1024;
-// 1: the planner gives the voxel-blocked kernel tensor-memory accumulators
-// where the frame block allows (8 or 16 frames), 0: registers
+// 1: the planner gives the voxel-blocked kernel tensor-memory accumulators,
+// 0: registers
 constexpr int VB_TMEM_DEFAULT = 1;
 // (with tensor-memory accumulators, vb = 2, followed by `zero_rows` staged
 // rows of zeros that lanes without a contribution read)
