@@ -355,17 +355,30 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
         if constexpr (TM) tm_zero();
 
-        // slabs are ordered by step s = tx * n_ele + rx, then frame block
-        auto slab = [&](int s) -> const char * { return S + ((int64_t)s * J.n_fb + fb) * J.slab_bytes; };
+        // Transmit order rotated per tile: a hash of the tile picks the
+        // quarter of the transmits the item starts from, so CTAs that share
+        // an SM run their per-step setup and their frame-pair FMAs out of
+        // phase rather than in lock step (started together, with equal step
+        // costs, they would stay aligned).  Whole transmits: per-transmit
+        // outputs stay complete.  The loop counter s stays the step's
+        // position in the item; eff(s) is the acquisition step it works on.
+        const int tx0 = g.n_tx >= 4 ? (int)((((uint32_t)tile * 0x9E3779B1u) >> 30) * (uint32_t)g.n_tx / 4u) : 0;
+        const int s0 = tx0 * g.n_ele;
+        auto eff = [&](int s) { const int e = s + s0; return e < n_steps ? e : e - n_steps; };
+        // slabs are ordered by step tx * n_ele + rx, then frame block
+        auto slab = [&](int s) -> const char * { return S + ((int64_t)eff(s) * J.n_fb + fb) * J.slab_bytes; };
         // (tx, rx) of step s: divided once per item, then advanced per step
         auto advance = [&](int &tx, int &rx) {
-            if (++rx == g.n_ele) { rx = 0; ++tx; }
+            if (++rx == g.n_ele) {
+                rx = 0;
+                if (++tx == g.n_tx) tx = 0;
+            }
         };
         auto window = [&](int s) -> VbWindow {
             VbWindow w;
             w.skip = true; w.lo = 0; w.count = 0; w.data = 0; w.overflow = false;
             if (s >= n_steps) return w;
-            return vb_window<KIND, D>(J, vb_ranges(J, s, n_steps, s / g.n_ele, s % g.n_ele, tu, tv, tz),
+            return vb_window<KIND, D>(J, vb_ranges(J, s, n_steps, eff(s) / g.n_ele, eff(s) % g.n_ele, tu, tv, tz),
                                       prm.wmax);
         };
         // rows [data, count) of a staged buffer hold zeros (shift rows past the record)
@@ -428,7 +441,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         };
 
         VbWindow wA = window(0), wB = window(1), wC;
-        int tx3 = 2 / g.n_ele, rx3 = 2 % g.n_ele;   // step of the ranges loaded next
+        int tx3 = eff(2 % n_steps) / g.n_ele, rx3 = eff(2 % n_steps) % g.n_ele;   // step of the ranges loaded next
         VbRanges rnext = vb_ranges(J, 2, n_steps, tx3, rx3, tu, tv, tz);   // ranges of the step two ahead
         advance(tx3, rx3);
         if constexpr (ASYNC) {
@@ -448,7 +461,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
         for (int v = 0; v < VB; ++v) { txi[v] = 0.f; txr[v] = 0.f; txq[v] = 0.f; }
         float4 enext = nvv > 0 ? __ldg(&g.rx_tab[rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
 
-        int tx = 0, rx = 0;   // of step s
+        int tx = tx0, rx = 0;   // of step s
         for (int s = 0; s < n_steps; ++s, advance(tx, rx)) {
             if constexpr (ASYNC) {
                 cp_async_wait<NST - 2>();

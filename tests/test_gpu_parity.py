@@ -359,6 +359,11 @@ def test_autotune_keeps_the_fastest_choice_and_the_result(bf, c2_small):
     torch.cuda.synchronize()
     assert H.rel_rms(after.cpu().numpy(), before.cpu().numpy()) < 1e-4
     if plan1["kernel"] == plan0["kernel"]:
-        assert torch.equal(after, before)   # tile and frame block change no arithmetic
+        if plan1["tile"] == plan0["tile"]:
+            assert torch.equal(after, before)   # the frame block changes no arithmetic
+        else:
+            # the tile sets the transmit order of the sums (voxel-blocked
+            # kernel): FP32 rounding only
+            assert H.rel_rms(after.cpu().numpy(), before.cpu().numpy()) < 1e-5
     print("autotune", res, "default plan", plan0)
     eng.close()
