@@ -19,8 +19,10 @@
 // rows hit distinct banks): cp.async for complex64 slabs, register staging
 // with one conversion for FP16/BF16 slabs.  Rows of the window past the end
 // of the record are zero-filled, so no load needs clamping.  The
-// interpolation weights come from degree-8 polynomials (weight_poly.h),
-// each mirrored pair of taps from one even and one odd chain.
+// interpolation weights come from polynomials (weight_poly.h; degree 8 for
+// complex64 slabs, degree 6 for FP16 / BF16 slabs, whose ~5e-4 relative
+// sample rounding is well above the degree-6 weight error of <= 8e-5), each
+// mirrored pair of taps from one even and one odd chain.
 //
 // TM variant: the 2 x VB x FB accumulator words of a thread (128 at FB = 16,
 // half the register file a thread can have) live in tensor memory instead
@@ -58,8 +60,9 @@ __device__ __forceinline__ float2 packed16_to_f2(uint32_t b, int store)
     return make_float2(__uint_as_float(b << 16), __uint_as_float(b & 0xffff0000u));
 }
 
-// Weights w[0..TAPS) at fractional offset d in [0, 1).
-template <int KIND>
+// Weights w[0..TAPS) at fractional offset d in [0, 1), from the degree-DEG
+// polynomials.
+template <int KIND, int DEG>
 __device__ __forceinline__ void poly_weights(float d, float (&w)[KindTraits<KIND>::TAPS])
 {
     if constexpr (KIND == K_QUAD3) {
@@ -70,19 +73,19 @@ __device__ __forceinline__ void poly_weights(float d, float (&w)[KindTraits<KIND
         // w_j(u) = E_j(u^2) + u O_j(u^2) and w_{T-1-j}(u) = w_j(-u) = E_j - u O_j:
         // both weights of a mirrored pair from one even and one odd Horner
         // chain in s = u^2 (DEG + 1 FMAs per pair)
-        using WP = WeightPoly<KIND>;
+        using WP = WeightPoly<KIND, DEG>;
         constexpr int T = KindTraits<KIND>::TAPS;
-        static_assert(WPOLY_DEG % 2 == 0, "even degree");
+        static_assert(DEG % 2 == 0, "even degree");
         const float u = fmaf(2.0f, d, -1.0f);
         const float s = u * u;
 #pragma unroll
         for (int j = 0; j < WP::HALF; ++j) {
-            float e = WP::c(j, WPOLY_DEG);
+            float e = WP::c(j, DEG);
 #pragma unroll
-            for (int m = WPOLY_DEG - 2; m >= 0; m -= 2) e = fmaf(e, s, WP::c(j, m));
-            float o = WP::c(j, WPOLY_DEG - 1);
+            for (int m = DEG - 2; m >= 0; m -= 2) e = fmaf(e, s, WP::c(j, m));
+            float o = WP::c(j, DEG - 1);
 #pragma unroll
-            for (int m = WPOLY_DEG - 3; m >= 1; m -= 2) o = fmaf(o, s, WP::c(j, m));
+            for (int m = DEG - 3; m >= 1; m -= 2) o = fmaf(o, s, WP::c(j, m));
             w[j] = fmaf(u, o, e);             // w_j(d)
             w[T - 1 - j] = fmaf(-u, o, e);    // w_{T-1-j}(d) = w_j(1 - d)
         }
@@ -149,7 +152,7 @@ __device__ __forceinline__ VbWindow vb_window(const FusedJob &J, const VbRanges 
 // (zeros elsewhere) and its complex factor P = apod * exp(j phase_tx) *
 // exp(j phase_rx) * exp(j phase_ab), zero for a voxel without a contribution
 // (its weights then multiply finite staged rows into an exact zero).
-template <int KIND, int D>
+template <int KIND, int D, int DEG>
 __device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&fl)[VB], const float (&dd)[VB],
                                          bool (&ok)[VB], float base, const float (&txr)[VB],
                                          const float (&txq)[VB], float4 e, float2 abp,
@@ -163,7 +166,7 @@ __device__ __forceinline__ void vb_terms(const FusedParams &prm, const float (&f
         if (ok[v] && o > D) { atomicAdd(prm.err_count, 1ull); ok[v] = false; }
         o = ok[v] ? o : 0;
         float w[TAPS];
-        poly_weights<KIND>(ok[v] ? dd[v] : 0.0f, w);   // finite whatever the index of a masked voxel
+        poly_weights<KIND, DEG>(ok[v] ? dd[v] : 0.0f, w);   // finite whatever the index of a masked voxel
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             float a = (k < TAPS) ? w[k] : 0.0f;
@@ -208,6 +211,11 @@ __device__ __forceinline__ void vb_pair_sums(const char *rows, const float (&ws)
 // fma.rn.f32x2; interleaved (re0, im0, re1, im1) for cp.async staging,
 // which copies complex64 slabs as they are.
 template <int STORE> struct VbPlanar { static constexpr bool value = STORE != ST_F32; };
+
+// Degree of the weight polynomials per slab storage: 8 for complex64
+// (weight error ~5e-7), 6 for FP16 / BF16 (weight error <= 8e-5, below the
+// ~5e-4 relative rounding of the stored samples).
+template <int STORE> struct VbWeightDeg { static constexpr int value = STORE == ST_F32 ? 8 : 6; };
 
 // (re, im) of frames 2p, 2p + 1 from a pair's four words in the layout
 template <bool PL>
@@ -508,7 +516,7 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                     if (base < 2.0e38f) {
                         float ws[VB][R];
                         float2 P[VB];
-                        vb_terms<KIND, D>(prm, fl, dd, ok, base, txr, txq, e, abp, ws, P);
+                        vb_terms<KIND, D, VbWeightDeg<STORE>::value>(prm, fl, dd, ok, base, txr, txq, e, abp, ws, P);
                         const int row0 = (int)base - KT::LO - wA.lo;
                         if (row0 < 0 || row0 + R > wA.count || wA.overflow) {
                             atomicAdd(prm.err_count, 1ull);   // never expected: window bound violated
@@ -564,7 +572,8 @@ fused_vb_kernel(const __grid_constant__ FusedParams prm)
                 if (__any_sync(0xffffffffu, use)) {
                     float ws[VB][R];
                     float2 P[VB];
-                    vb_terms<KIND, D>(prm, fl, dd, ok, use ? base : 0.0f, txr, txq, e, abp, ws, P);
+                    vb_terms<KIND, D, VbWeightDeg<STORE>::value>(prm, fl, dd, ok, use ? base : 0.0f, txr, txq, e, abp, ws,
+                                                                 P);
                     const char *rows = reinterpret_cast<const char *>(stages) +
                                        (use ? (s % NST) * stage_bytes + row0 * STRIDE : zero_off);
                     __syncwarp();     // converged after the divergent checks above
