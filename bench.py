@@ -43,7 +43,8 @@ METRIC = "DAS voxel·rx·tx/s (nominal, summed over frames)"
 UNIT = "voxel·rx·tx/s"
 # plan kernel -> CUDA kernel function
 KERNEL_NAMES = {"fused_voxel_blocked": "fused_vb_kernel", "fused_voxel_blocked_tmem": "fused_vb_kernel",
-                "fused": "fused_das_kernel", "plain": "plain_das_kernel"}
+                "fused": "fused_das_kernel", "plain": "plain_das_kernel", "fused_tensor_core": "fused_tc_kernel",
+                "fused_tensor_core_fp16w": "fused_tc_kernel"}
 
 
 def parse():
@@ -55,9 +56,10 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--frames", type=int, default=None, help="override the workload's frame count (profiling cases)")
     ap.add_argument("--storage", default=None, help="float32 | float16 | bfloat16 (default: workload's)")
-    ap.add_argument("--kernel", default="fused", choices=["fused", "plain", "tmem", "regs"],
+    ap.add_argument("--kernel", default="fused", choices=["fused", "plain", "tmem", "regs", "tc", "tc16"],
                     help="fused: the planner's (or autotuner's) choice; tmem / regs: the voxel-blocked kernel "
-                         "with tensor-memory / register accumulators")
+                         "with tensor-memory / register accumulators; tc / tc16: the tensor-core kernel with "
+                         "hi + remainder / single FP16 weights")
     ap.add_argument("--frames-per-block", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -72,6 +74,9 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
     ap.add_argument("--plain-frames", type=int, default=10)
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference kernel on the GPU")
+    ap.add_argument("--ref-gpu-frames", type=int, default=20,
+                    help="frames of the workload the reference GPU kernel is timed on")
     ap.add_argument("--cpu-sample-frames", type=int, default=4)
     ap.add_argument("--cpu-sample-z", type=int, default=8)
     return ap.parse_args()
@@ -369,6 +374,38 @@ def simulator_leg(dev, seed: int = 7):
             "note": "scatterers static within a frame: one element field per frame, all transmits as one GEMM"}
 
 
+def ref_gpu_leg(w, data, frames: int, variant: str = "fast"):
+    """The reference's own CUDA kernel on this GPU (bfVirtualSourceGeneric_RCA.cu
+    compiled from its source; "fast" = -use_fast_math, as the reference
+    wrapper builds it at bfVirtualSourceGeneric_RCA.m:796), launched the way
+    the wrapper launches it (block 1024, grid [ceil(nPix/1024), nTx,
+    nFrameChunk], frames chunked per .m:587-594, compounding sum over
+    transmits on the device per .m:689-697), channel data resident on the
+    device, on the first ``frames`` frames; rate in voxel.rx.tx/s.  Both of
+    the reference's interpolation kernels are timed: its 6-tap "Lanczos
+    5-lobes" option and its default quadratic."""
+    from oracle import host as H
+    from simu_rca_ab_b200 import workloads as W
+
+    if not H.have_ref_gpu(variant):
+        return {"unavailable": f"oracle/_ref/librca_ref_gpu_{variant}.so not built"}
+    res = {"kernel": f"reference bfVirtualSourceGeneric_RCA.cu, sm_100a, {variant} build"
+                     + (" (-use_fast_math, as the reference wrapper compiles it)" if variant == "fast" else ""),
+           "frames": frames}
+    for name, lz in (("ref6", True), ("quadratic", False)):
+        ms, units, chunks = 0.0, 0, 0
+        for gi, g in enumerate(w.groups):
+            d = W.group_data(w, data[:frames], gi).cpu().numpy()
+            r = H.prepare(W.as_matlab(d), g.Geometry, g.Transmit, w.Param,
+                          {"flagInterpolationLanczos": lz, "flagCompounding": True, "flagMaskTransmit": False})
+            t, nc = H.time_ref_gpu(r, variant)
+            ms += t
+            chunks += nc
+            units += r.n_pix * r.n_ch * r.n_tx * r.n_frame
+        res[name] = {"value": units / (ms * 1e-3), "unit": UNIT, "ms": ms, "launches": chunks}
+    return res
+
+
 def run_reference(a, rank):
     """--impl reference: the reference's own kernel source on the host cores."""
     if rank != 0:
@@ -433,8 +470,8 @@ def main():
     w = W.get(a.workload, n_frame=a.frames)
     storage = a.storage or w.storage
     st_code = {"float32": L.STORE_F32, "float16": L.STORE_F16, "bfloat16": L.STORE_BF16}[storage]
-    kern = {"plain": L.KERNEL_PLAIN, "tmem": L.KERNEL_FUSED_TMEM, "regs": L.KERNEL_FUSED_REGS}.get(a.kernel,
-                                                                                                 L.KERNEL_FUSED)
+    kern = {"plain": L.KERNEL_PLAIN, "tmem": L.KERNEL_FUSED_TMEM, "regs": L.KERNEL_FUSED_REGS,
+            "tc": L.KERNEL_FUSED_TC, "tc16": L.KERNEL_FUSED_TC_FP16W}.get(a.kernel, L.KERNEL_FUSED)
 
     data = W.channel_data(w, seed=rank, device=dev)                       # [F][T][E][S] complex64
     in_dtype = torch.complex32 if storage == "float16" else torch.complex64
@@ -648,6 +685,18 @@ def main():
                  "ratio": (value / world) / p_val}
         del p_in, p_out
 
+    ref_gpu = None
+    if not a.no_ref_gpu and rank == 0:
+        try:
+            ref_gpu = ref_gpu_leg(w, data, max(1, min(a.ref_gpu_frames, F)))
+            for k in ("ref6", "quadratic"):
+                if k in ref_gpu:
+                    ref_gpu[k]["ratio"] = (value / world) / ref_gpu[k]["value"]
+        except Exception as ex:
+            ref_gpu = {"error": f"{type(ex).__name__}: {ex}"}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
     serving = None
     if not a.no_serving and rank == 0:
         try:
@@ -725,7 +774,7 @@ def main():
                        "units_per_step": units, "parallelism": f"weak x{world} (independent ensembles)",
                        "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain,
+            "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain, "reference_gpu": ref_gpu,
             "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim, "ulm": ulm,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }

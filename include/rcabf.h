@@ -124,7 +124,17 @@ typedef enum rcabf_kernel {
        (RCABF_ERR_UNSUPPORTED where the geometry allows no voxel blocking):
        tensor memory (sm_100a TMEM) or registers */
     RCABF_KERNEL_FUSED_TMEM = 4,
-    RCABF_KERNEL_FUSED_REGS = 5
+    RCABF_KERNEL_FUSED_REGS = 5,
+    /* the tensor-core kernel (sm_100a tcgen05.mma: each (tx, element) step of
+       a 128-voxel tile is a banded product of the voxels' interpolation
+       weights with the sample window of all frames of a block, accumulated
+       in tensor memory over the acquisition): FP16 storage, exact tables,
+       compounded output, rectilinear grids, at least 32 frames.  Weights
+       enter the MMA as an FP16 value plus its FP16 remainder (~22 bits;
+       products exact, sums FP32) -- or, with _FP16W, as one FP16 value
+       (~11 bits, half the tensor work) */
+    RCABF_KERNEL_FUSED_TC = 6,
+    RCABF_KERNEL_FUSED_TC_FP16W = 7
 } rcabf_kernel;
 
 /* ------------------------------------------------------------------------ */
@@ -286,7 +296,10 @@ int rcabf_beamform_host(const rcabf_geometry *g, const rcabf_beamform_args *a, i
  * needs more than RCABF_NOALLOC_WORKSPACE_BYTES, and with
  * RCABF_ERR_UNSUPPORTED when the plan is the plain kernel.  All calls on one
  * device share the array: calls that overlap in time (other streams, other
- * threads) race and must be serialised by the caller. */
+ * threads) race and must be serialised by the caller.  Each call checks
+ * that the geometry's device is the current device (RCABF_ERR_INVALID_ARGUMENT
+ * otherwise).  The looked-up addresses are kept for the life of the process:
+ * do not call cudaDeviceReset while the library is loaded. */
 int rcabf_beamform_noalloc(const rcabf_geometry *g, const rcabf_beamform_args *a, void *stream);
 
 /* What rcabf_autotune chose for a geometry, frame count and storage. */

@@ -332,6 +332,52 @@ def run_ref_gpu(r: RefArgs, variant: str = "strict", kernel: str = "base", ab_la
     return out, mask
 
 
+def time_ref_gpu(r: RefArgs, variant: str = "fast", iters: int = 2, warmup: int = 1):
+    """Times O2 -- the reference kernel on the GPU -- the way the reference
+    wrapper runs it (bfVirtualSourceGeneric_RCA.m:587-594 frame chunks so that
+    2*nPix*nTx*nFrame < 2^31, .m:640-650 launch shape, .m:689-697 compounding
+    sum over transmits on the device), with the channel data already resident
+    on the device.  Returns (ms per run over all of r's frames, chunks)."""
+    import torch
+    L = _load(LIB_REF_GPU[variant])
+    L.rca_ref_gpu_launch.restype = C.c_int
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    tens = {k: t(getattr(r, k)) for k in ("gx", "gy", "gz", "ex", "ey", "ez", "vsx", "vsy", "vsz", "min_dist")}
+    dptr = {k: C.cast(C.c_void_p(v.data_ptr()), _f) for k, v in tens.items()}
+    n_chunks = int(np.ceil(2 * r.n_pix * r.n_tx * r.n_frame / (2 ** 31 - 1)))
+    bounds = np.round(np.linspace(0, r.n_frame, n_chunks + 1)).astype(int)
+    fmax = int(np.max(np.diff(bounds)))
+    data_d = t(r.data)
+    mask_d = torch.zeros((r.n_tx, r.n_pix), dtype=torch.float32, device=dev)
+    ob = torch.empty((fmax, r.n_tx, r.n_pix, 2), dtype=torch.float32, device=dev)
+    comp = torch.empty((r.n_frame, r.n_pix, 2), dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream()
+
+    def run():
+        for k in range(n_chunks):
+            f0, f1 = int(bounds[k]), int(bounds[k + 1])
+            d = C.cast(C.c_void_p(data_d[f0:f1].data_ptr()), _f)
+            args = _kernel_args(r, d, C.cast(C.c_void_p(ob.data_ptr()), _f),
+                                C.cast(C.c_void_p(mask_d.data_ptr()), _f), dptr)
+            args.insert(-1, None)
+            args += [C.c_int(r.n_pix), C.c_int(r.n_ch), C.c_int(r.n_tx), C.c_int(f1 - f0), C.c_int(r.n_sample),
+                     C.c_int(int(r.lanczos)), C.c_int(int(r.mask_transmit)), C.c_void_p(st.cuda_stream)]
+            assert L.rca_ref_gpu_launch(*args) == 0
+            torch.sum(ob[: f1 - f0], dim=1, out=comp[f0:f1])
+
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(iters):
+        run()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / iters, n_chunks
+
+
 def compound(per_tx: np.ndarray, mask_tx: np.ndarray, compounding: bool = True):
     """RCA.m:689-697: sum over transmits (sequential, single precision)."""
     if not compounding:

@@ -19,6 +19,7 @@ GRID_RECTILINEAR, GRID_POINTS = 0, 1
 IQ_C64, IQ_C32, IQ_BF16X2, IQ_RF_F32 = 0, 1, 2, 3
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 KERNEL_AUTO, KERNEL_FUSED, KERNEL_PLAIN, KERNEL_FUSED_NOBLOCK, KERNEL_FUSED_TMEM, KERNEL_FUSED_REGS = 0, 1, 2, 3, 4, 5
+KERNEL_FUSED_TC, KERNEL_FUSED_TC_FP16W = 6, 7
 
 OK = 0
 ERR_UNSUPPORTED = 102

@@ -133,9 +133,10 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     if (a->storage < RCABF_STORE_F32 || a->storage > RCABF_STORE_BF16) return RCABF_ERR_INVALID_ARGUMENT;
     if (g->mode == MODE_REF && a->storage != RCABF_STORE_F32) return RCABF_ERR_UNSUPPORTED;
     const int fb_req = a->frames_per_block;
-    if (fb_req != 0 && !fb_supported(g->mode, fb_req)) return RCABF_ERR_INVALID_ARGUMENT;
+    const bool tc_req = a->kernel == RCABF_KERNEL_FUSED_TC || a->kernel == RCABF_KERNEL_FUSED_TC_FP16W;
+    if (fb_req != 0 && !tc_req && !fb_supported(g->mode, fb_req)) return RCABF_ERR_INVALID_ARGUMENT;
     if (a->per_channel && a->compound) return RCABF_ERR_INVALID_ARGUMENT;   // no sum over elements: none over tx
-    if (a->kernel < RCABF_KERNEL_AUTO || a->kernel > RCABF_KERNEL_FUSED_REGS) return RCABF_ERR_INVALID_ARGUMENT;
+    if (a->kernel < RCABF_KERNEL_AUTO || a->kernel > RCABF_KERNEL_FUSED_TC_FP16W) return RCABF_ERR_INVALID_ARGUMENT;
     p = Plan{};
     p.kernel = (a->kernel == RCABF_KERNEL_PLAIN || a->per_channel) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
     if (p.kernel == RCABF_KERNEL_PLAIN) {
@@ -149,9 +150,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
         std::lock_guard<std::mutex> lk(g->mu);
         auto it = g->tuned.find({a->n_frame, (int64_t)a->storage});
         const int vb_req = a->kernel == RCABF_KERNEL_FUSED_TMEM ? 2 : a->kernel == RCABF_KERNEL_FUSED_REGS ? 1 : -1;
-        if (it != g->tuned.end() && (fb_req == 0 || fb_req == it->second.fb) &&
-            !(it->second.vb && a->kernel == RCABF_KERNEL_FUSED_NOBLOCK) &&
-            (vb_req < 0 || vb_req == it->second.vb)) {
+        if (it != g->tuned.end() && !tc_req && (fb_req == 0 || fb_req == it->second.fb) &&
+            !((it->second.vb || it->second.tc) && a->kernel == RCABF_KERNEL_FUSED_NOBLOCK) &&
+            !(it->second.tc && (vb_req >= 0 || !a->compound)) && (vb_req < 0 || vb_req == it->second.vb)) {
             tuned = it->second;
             force = &tuned;
         }
@@ -162,7 +163,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
         p.tiles_u = (int)((g->n_u + p.ts.tu - 1) / p.ts.tu);
         p.tiles_v = (int)((g->n_v + tile_v_extent - 1) / tile_v_extent);
         p.row_words = fused_row_words(p.fb);
-        p.slab_bytes = ((int64_t)a->n_sample * p.fb * es + 15) / 16 * 16;
+        p.slab_bytes = ((int64_t)(p.tc ? p.tc_rows : a->n_sample) * p.fb * es + 15) / 16 * 16;
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
         size_t off = 0;
         p.off_S = off;
@@ -174,6 +175,46 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
         p.total = off;
         p.n_items = (int64_t)p.n_fb * p.tiles_z * p.tiles_u * p.tiles_v;
     };
+
+    // Tensor-core kernel: FP16 slabs, exact tables, compounded output, a
+    // rectilinear grid whose 4 x 32 x 1 tiles need windows of at most 32
+    // rows, at least 32 frames; frame blocks of a multiple of 8 frames, as
+    // few as the tensor-memory budget allows (the weights are built once
+    // per block).
+    const int want_tc = force ? force->tc
+                        : a->kernel == RCABF_KERNEL_FUSED_TC       ? 2
+                        : a->kernel == RCABF_KERNEL_FUSED_TC_FP16W ? 1
+                                                                   : 0;
+    if (want_tc) {
+        const TileShape tts{TC_TILE_U, TC_TILE_V, 1};
+        const int fbmax = tc_max_frames_per_block(want_tc == 2);
+        bool ok = g->mode == MODE_EXACT && a->storage == RCABF_STORE_F16 && a->compound && !a->per_channel &&
+                  g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_frame >= 32 && a->n_sample >= 2 &&
+                  g->window_rows(tts) <= TC_MAX_ROWS;
+        int fb = 0;
+        if (ok) {
+            const int64_t nfb = (a->n_frame + fbmax - 1) / fbmax;
+            fb = std::max<int>(32, (int)(((a->n_frame + nfb - 1) / nfb + 7) / 8 * 8));
+            if (force && force->fb) fb = force->fb;
+            else if (fb_req > 0) fb = fb_req;
+            ok = fb >= 32 && fb <= fbmax && fb % 8 == 0;
+        }
+        if (ok) {
+            p.tc = want_tc;
+            p.fb = fb;
+            p.ts = tts;
+            p.tc_rows = (int)a->n_sample + TC_MAX_ROWS;
+            layout(tts.tv);
+            ok = (int64_t)g->n_tx * g->n_ele * p.n_fb * p.tc_rows < ((int64_t)1 << 31);
+        }
+        if (ok) {
+            p.wmax = TC_MAX_ROWS;
+            p.smem = tc_launch_smem(fb);
+            return RCABF_OK;
+        }
+        p = Plan{};
+        return RCABF_ERR_UNSUPPORTED;
+    }
 
     // Voxel-blocked kernel: exact tables, a steering axis to block along,
     // frames in pairs, and at most 2 rows of shift inside a block.  Its
@@ -266,7 +307,7 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
     IngestParams ip{};
     ip.iq = a->iq; ip.iq_dtype = a->iq_dtype; ip.n_sample = (int)a->n_sample; ip.n_ele = g->n_ele;
     ip.n_tx = g->n_tx; ip.n_frame = a->n_frame; ip.fb = p.fb; ip.n_fb = p.n_fb;
-    ip.S = ws + p.off_S; ip.slab_bytes = p.slab_bytes;
+    ip.S = ws + p.off_S; ip.slab_bytes = p.slab_bytes; ip.n_rows = p.tc ? p.tc_rows : 0;
     cudaError_t ce = launch_ingest(ip, p.store, st);
     if (ce != cudaSuccess) return cuda_fail(ce, "ingest launch");
     if (marks) mark(marks, 1, st);
@@ -326,6 +367,16 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     // a counter set by the caller (rcabf_beamform_noalloc) is kept
     DeviceState *ds = device_state(g0->device, prm.err_count == nullptr);
     if (!prm.err_count) prm.err_count = ds->err;
+    if (p.tc) {   // one launch per job (a persistent grid of one CTA per SM each)
+        for (int j = 0; j < prm.n_jobs; ++j) {
+            const int64_t end = j + 1 < prm.n_jobs ? prm.jobs[j + 1].item_begin : prm.n_items;
+            const cudaError_t le = launch_fused_tc(g0->kind, p.tc == 2, prm.jobs[j], p.fb, p.tc_rows,
+                                                   end - prm.jobs[j].item_begin, prm.err_count, ds->n_sm, st);
+            if (le != cudaSuccess) return cuda_fail(le, "tensor-core kernel launch");
+            g_launches += 1;
+        }
+        return RCABF_OK;
+    }
     const size_t smem = p.vb ? vb_smem_bytes(p.store, prm.wmax, prm.row_words,
                                              p.vb == 2 ? kind_taps(g0->kind) + p.d : 0)
                              : fused_smem_bytes(g0->mode, g0->kind, p.store, prm.wmax, prm.row_words);
@@ -405,7 +456,9 @@ static int beamform_planned(rcabf_geometry *g, const rcabf_beamform_args *a, con
 }
 
 // Static workspace of rcabf_beamform_noalloc, per device: looked up once with
-// the device current, its error counter cleared then.
+// the device current, its error counter cleared then.  Every call checks that
+// the geometry's device is the current one before it uses the cached
+// addresses: they are device addresses of that GPU only.
 struct NoallocRegion {
     void *ws = nullptr;
     unsigned long long *err = nullptr;
@@ -415,18 +468,18 @@ static std::map<int, NoallocRegion> g_noalloc;
 
 static int noalloc_setup(int dev, NoallocRegion &r, bool create)
 {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return cuda_fail(e, "noalloc: cudaGetDevice");
+    if (cur != dev) {
+        snprintf(g_last_err, sizeof(g_last_err),
+                 "noalloc: the geometry's device %d is not the current device %d", dev, cur);
+        return RCABF_ERR_INVALID_ARGUMENT;
+    }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     auto it = g_noalloc.find(dev);
     if (it != g_noalloc.end()) { r = it->second; return RCABF_OK; }
     if (!create) return RCABF_ERR_PENDING;
-    int cur = -1;
-    cudaError_t e = cudaGetDevice(&cur);
-    if (e != cudaSuccess) return cuda_fail(e, "noalloc set-up: cudaGetDevice");
-    if (cur != dev) {
-        snprintf(g_last_err, sizeof(g_last_err),
-                 "noalloc set-up: the geometry's device %d is not the current device %d", dev, cur);
-        return RCABF_ERR_INVALID_ARGUMENT;
-    }
     NoallocRegion n;
     if ((e = noalloc_region(&n.ws, &n.err)) != cudaSuccess) return cuda_fail(e, "noalloc set-up: cudaGetSymbolAddress");
     if ((e = cudaMemset(n.err, 0, sizeof(unsigned long long))) != cudaSuccess)
@@ -586,11 +639,15 @@ int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, c
     int s = plan_beamform(const_cast<rcabf_geometry *>(g), a, p);
     if (s != RCABF_OK) return s;
     int occ = 0;   // resident CTAs per SM of the fused kernel (0: plain kernel)
-    if (p.kernel == RCABF_KERNEL_FUSED) {
+    if (p.tc) {
+        occ = 1;
+    } else if (p.kernel == RCABF_KERNEL_FUSED) {
         s = resident_ctas(g, p, p.smem, device_state(g->device), occ);
         if (s != RCABF_OK) return s;
     }
     const char *kname = p.kernel == RCABF_KERNEL_PLAIN ? "plain"
+                        : p.tc == 2                     ? "fused_tensor_core"
+                        : p.tc == 1                     ? "fused_tensor_core_fp16w"
                         : p.vb == 2                     ? "fused_voxel_blocked_tmem"
                         : p.vb                          ? "fused_voxel_blocked"
                                                         : "fused";

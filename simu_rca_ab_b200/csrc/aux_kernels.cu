@@ -1,5 +1,7 @@
 // Auxiliary kernels of librcabf: channel-data ingest, per-tile window range
 // tables, the apodisation-sum mask, and an FP32 FMA throughput probe.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -46,17 +48,18 @@ __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p)
     __syncthreads();
     T *slab = reinterpret_cast<T *>(reinterpret_cast<char *>(p.S) +
                                     (((int64_t)tx * p.n_ele + ele) * p.n_fb + fb) * p.slab_bytes);
+    const int n_rows = max(p.n_rows, p.n_sample);
     for (int i = threadIdx.x; i < FB * INGEST_NS; i += blockDim.x) {
         const int nl = i / FB, fi = i % FB;
         const int n = n_base + nl;
-        if (n < p.n_sample) slab[(int64_t)n * FB + fi] = from_f2<STORE>(tile[fi][nl]);
+        if (n < n_rows) slab[(int64_t)n * FB + fi] = from_f2<STORE>(tile[fi][nl]);   // zeros past the record
     }
 }
 
 template <int STORE>
 static cudaError_t launch_ingest_store(const IngestParams &p, cudaStream_t st)
 {
-    dim3 grid((p.n_sample + INGEST_NS - 1) / INGEST_NS, p.n_fb, p.n_tx * p.n_ele);
+    dim3 grid((std::max(p.n_rows, p.n_sample) + INGEST_NS - 1) / INGEST_NS, p.n_fb, p.n_tx * p.n_ele);
     switch (p.iq_dtype) {
     case 0: ingest_kernel<STORE, 0><<<grid, 256, 0, st>>>(p); break;
     case 1: ingest_kernel<STORE, 1><<<grid, 256, 0, st>>>(p); break;

@@ -1,0 +1,103 @@
+// Tensor-core delay-and-sum kernel (fused_tc_kernel.cuh): instantiations,
+// the slab tensor map and the launch.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "fused_tc_kernel.cuh"
+#include "launchers.h"
+
+namespace rcabf {
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the
+// runtime (no link-time dependency on libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+template <int KIND, bool SPLIT>
+static cudaError_t tc_do(const TcParams *p, int grid, size_t smem, cudaStream_t st, int what)
+{
+    auto k = fused_tc_kernel<KIND, SPLIT>;
+    if (what == 1) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<grid, TC_THREADS, smem, st>>>(*p);
+    return cudaGetLastError();
+}
+
+template <int KIND>
+static cudaError_t tc_split(bool split, const TcParams *p, int grid, size_t smem, cudaStream_t st, int what)
+{
+    return split ? tc_do<KIND, true>(p, grid, smem, st, what) : tc_do<KIND, false>(p, grid, smem, st, what);
+}
+
+static cudaError_t tc_route(int kind, bool split, const TcParams *p, int grid, size_t smem, cudaStream_t st,
+                            int what)
+{
+    switch (kind) {
+    case K_QUAD3: return tc_split<K_QUAD3>(split, p, grid, smem, st, what);
+    case K_REF6: return tc_split<K_REF6>(split, p, grid, smem, st, what);
+    case K_LANCZOS2: return tc_split<K_LANCZOS2>(split, p, grid, smem, st, what);
+    case K_LANCZOS3: return tc_split<K_LANCZOS3>(split, p, grid, smem, st, what);
+    case K_LANCZOS4: return tc_split<K_LANCZOS4>(split, p, grid, smem, st, what);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t tc_launch_smem(int fb)
+{
+    // at least half of an SM's shared memory, so that one CTA holds an SM
+    // (the kernel allocates all 512 tensor-memory columns)
+    return std::max<size_t>(tc_smem_bytes(fb), 116 * 1024);
+}
+
+int tc_max_frames_per_block(int split) { return tc_max_fb(split != 0); }
+int tc_tmem_columns(int fb, int split) { return tc_tmem_cols(fb, split != 0); }
+
+cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, int rows_per_slab, int64_t n_items,
+                            unsigned long long *err, int n_sm, cudaStream_t st)
+{
+    if (fb < 32 || fb > tc_max_fb(split != 0) || (fb & 7) || tc_tmem_cols(fb, split != 0) > 512)
+        return cudaErrorInvalidValue;
+    const int64_t rows = (int64_t)job.g.n_tx * job.g.n_ele * job.n_fb * rows_per_slab;
+    if (rows >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    auto enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    TcParams p{};
+    p.job = job;
+    p.fb = fb;
+    p.rows_per_slab = rows_per_slab;
+    p.n_items = n_items;
+    p.err_count = err;
+    // the slabs as one 2-D FP16 tensor: rows of 2 fb halfs, one box = 64
+    // halfs x 16 rows, 128-byte swizzle (the MMA's B layout); columns past
+    // 2 fb (the last panel) read as zeros
+    cuuint64_t dims[2] = {(cuuint64_t)(2 * fb), (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(4 * fb)};
+    cuuint32_t box[2] = {64, 16};
+    cuuint32_t es[2] = {1, 1};
+    const CUresult cr = enc(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(job.S), dims, strides, box,
+                            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const size_t smem = tc_launch_smem(fb);
+    if (job.g.mode != MODE_EXACT || !job.compound) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = tc_route(kind, split != 0, nullptr, 0, smem, nullptr, 1)) != cudaSuccess) return e;
+    const int grid = (int)std::min<int64_t>(n_items, n_sm);
+    if (grid <= 0) return cudaSuccess;
+    return tc_route(kind, split != 0, &p, grid, smem, st, 0);
+}
+
+}  // namespace rcabf

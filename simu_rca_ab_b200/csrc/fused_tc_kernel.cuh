@@ -1,0 +1,483 @@
+// Delay-and-sum on the tensor cores (sm_100a tcgen05.mma), EXACT tables,
+// FP16 slabs, rectilinear grids, transmits compounded.
+//
+// Formulation.  For a tile of 128 voxels (TU along the receive axis x TV
+// along the steering axis, one depth) and one (tx, rx) step, the sample
+// rows every voxel of the tile touches form one window [lo, lo + K) of the
+// step's slab, K <= 32 rows.  With W[m][k] = P_m w_m(k - o_m) (the voxel's
+// interpolation weights placed at its own row offset o_m inside the window,
+// times its complex factor P = apod * transmit phasor * receive phasor), the
+// step's contribution to every frame f is a banded matrix product
+//     out[m][f] += sum_k W[m][k] * S[lo + k][f],
+// and summing over all (tx, rx) steps is one long contraction: the tile's
+// accumulators stay in tensor memory across the whole acquisition.  S rows
+// hold the frames of a block as (re, im) FP16 pairs, so with the real and
+// imaginary parts of W in two matrices,
+//     D_r = Re(W) . S,  D_i = Im(W) . S    (N = 2 FB columns, (re, im) per frame)
+//     out_re = D_r[re] - D_i[im],  out_im = D_r[im] + D_i[re].
+// Weights are formed in FP32 exactly as the SIMT kernels form them (degree-6
+// polynomials, FP32 phasors) and enter the MMA as FP16: SPLIT = true adds a
+// second FP16 term holding the remainder (hi + lo carries ~22 bits, the MMA
+// products are exact and summed in FP32), SPLIT = false keeps the single
+// FP16 rounding (~11 bits).  All weights are scaled by 2^8 (undone in the
+// epilogue) so that the remainder terms stay out of the FP16 subnormal range.
+//
+// Roles (192 threads): warps 0-3 build the weight matrices, one voxel per
+// thread, straight into tensor memory (lane = voxel row; tcgen05.st), and
+// write the outputs; warp 4 computes the windows of 32 steps at a time and
+// loads each active step's window with 2-D TMA (128-byte swizzle) into a
+// ring of NS shared-memory stages; warp 5 issues the MMAs (A from tensor
+// memory, B from shared memory) and commits them to the stage's "empty"
+// barrier.  Steps whose window is empty for the whole tile are skipped by
+// every role alike: the producer passes each active step's record (step,
+// window start, 16-row chunks) through the stage ring, followed by an
+// end-of-item record.  Every wait is bounded (mbar_wait): a wait that runs
+// out sets an abort flag, counts an error and every role leaves its loop.
+//
+// Tensor memory (512 columns, one CTA per SM): D_r at column 0, D_i at
+// column N16, then NS stages of NMAT weight matrices of 16 columns (32 FP16
+// per row: K <= 32).
+#pragma once
+
+#include <cuda.h>
+
+#include "das_common.cuh"
+#include "poly_weights.cuh"
+#include "tc_common.cuh"
+
+namespace rcabf {
+
+constexpr int TC_THREADS = 192;
+constexpr int TC_TU = TC_TILE_U, TC_TV = TC_TILE_V;   // tile: TU (receive axis) x TV (steering axis) x 1 depth
+constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
+static_assert(TC_TU * TC_TV == 128, "one voxel per tensor-memory lane");
+constexpr int TC_NS = 3;                   // pipeline stages
+constexpr int TC_PANEL_BYTES = TC_KCH * 2048;   // one 64-element panel of B: TC_KCH x (16 rows x 128 B)
+constexpr float TC_SCALE = 256.0f;
+constexpr RCABF_HD int tc_nmat(bool split) { return split ? 4 : 2; }
+constexpr RCABF_HD int tc_n16(int fb) { return (2 * fb + 15) / 16 * 16; }
+constexpr RCABF_HD int tc_panels(int fb) { return (2 * fb + 63) / 64; }
+// tensor-memory columns the kernel needs at frame block fb
+constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return 2 * tc_n16(fb) + TC_NS * (split ? 4 : 2) * 16; }
+// largest frame block that fits the 512 columns
+constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 80 : 104; }
+// dynamic shared memory: NS stages of B panels + 1 KB for the 1024-byte alignment
+constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NS * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+
+// All lanes wait on the barrier; the warp proceeds (converged) only if every
+// lane saw the phase complete.
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
+{
+    const bool ok = mbar_wait(bar, parity, abort);
+    return __all_sync(0xffffffffu, ok);
+}
+
+struct TcInfo {
+    int32_t s, lo, nk, end;
+};
+// a record written by another thread (published through an mbarrier)
+__device__ __forceinline__ TcInfo read_info(const TcInfo *p)
+{
+    const volatile TcInfo *v = p;
+    TcInfo r;
+    r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.end = v->end;
+    return r;
+}
+
+struct TcParams {
+    CUtensorMap tmap;           // slab rows: dim 0 = 2 FB halfs (a row), dim 1 = rows of all slabs
+    FusedJob job;
+    int32_t fb;                 // frames per block (multiple of 8, 32..tc_max_fb)
+    int32_t rows_per_slab;      // n_sample + 32 (zero rows past the record)
+    int64_t n_items;            // n_fb * tiles
+    unsigned long long *err_count;
+};
+
+// One step's window for the tile (producer): rows [lo, lo + 16 nk) of the
+// step's slab cover every tap of every voxel of the tile.
+template <int KIND>
+__device__ __forceinline__ bool tc_window(const FusedJob &J, int s, int tx, int rx, int tu, int tv, int tz, int &lo,
+                                          int &nk, bool &overflow)
+{
+    using KT = KindTraits<KIND>;
+    overflow = false;
+    const float2 rr = J.rx_range[((int64_t)rx * J.tiles_u + tu) * J.tiles_z + tz];
+    const float2 tr = J.tx_range[((int64_t)tx * J.tiles_v + tv) * J.tiles_z + tz];
+    if (!(rr.x <= rr.y) || !(tr.x <= tr.y)) return false;
+    const float ab = ab_value(J.g, tx, rx);
+    float lo_f = __fadd_rn(__fadd_rn(tr.x, rr.x), ab);
+    float hi_f = __fadd_rn(__fadd_rn(tr.y, rr.y), ab);
+    const float fmax_n = (float)J.n_sample;
+    lo_f = fminf(fmaxf(floorf(lo_f), -1.0f), fmax_n);
+    hi_f = fminf(fmaxf(floorf(hi_f), -1.0f), fmax_n);
+    int l = max((int)lo_f - KT::LO, 0);
+    const int h = min((int)hi_f - KT::LO + KT::TAPS - 1, J.n_sample - 2);
+    if (h < l) return false;
+    const int count = h - l + 1;
+    nk = (count + 15) >> 4;
+    if (nk > TC_KCH) { overflow = true; return false; }
+    lo = l;
+    (void)s;
+    return true;
+}
+
+// The TAPS weights shifted to start at position o of an NP-position row
+// (positions outside the taps are zero): a barrel shifter of log2(NP)
+// select stages, so that no register is indexed at run time.
+template <int TAPS, int NP>
+__device__ __forceinline__ void tc_place(const float (&w)[TAPS], int o, float (&v)[NP])
+{
+#pragma unroll
+    for (int p = 0; p < NP; ++p) v[p] = p < TAPS ? w[p] : 0.0f;
+#pragma unroll
+    for (int b = 1; b < NP; b <<= 1) {
+        const bool on = (o & b) != 0;
+#pragma unroll
+        for (int p = NP - 1; p >= 0; --p) v[p] = on ? (p >= b ? v[p - b] : 0.0f) : v[p];
+    }
+}
+
+// FP32 values -> packed FP16 pairs (even index in the low half): the value's
+// rounding (hi) and, for SPLIT, the rounding of the remainder (lo).
+__device__ __forceinline__ uint32_t tc_pack(float a, float b)
+{
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+__device__ __forceinline__ uint32_t tc_pack_rem(float a, float b, uint32_t hi)
+{
+    __half2 h = *reinterpret_cast<__half2 *>(&hi);
+    const float2 f = __half22float2(h);
+    return tc_pack(a - f.x, b - f.y);
+}
+
+template <int KIND, bool SPLIT>
+__global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_constant__ TcParams prm)
+{
+    using KT = KindTraits<KIND>;
+    constexpr int TAPS = KT::TAPS;
+    constexpr int NMAT = tc_nmat(SPLIT);
+    const FusedJob &J = prm.job;
+    const DevGeom &g = J.g;
+    const int FB = prm.fb;
+    const int NH = 2 * FB;                 // halfs per slab row = MMA N
+    const int N16 = tc_n16(FB);
+    const int NP = tc_panels(FB);
+    const int stage_bytes = NP * TC_PANEL_BYTES;
+    const int a_col0 = 2 * N16;            // first weight-matrix column
+    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
+
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint64_t full_b[TC_NS], full_a[TC_NS], empty[TC_NS];
+    __shared__ uint64_t acc_full, acc_empty, fin;
+    __shared__ TcInfo info[TC_NS];
+    __shared__ uint32_t tbase_s;
+    __shared__ volatile int abort_s;
+    uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        unsigned dyn;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        if (dyn < (unsigned)tc_smem_bytes(FB) || tc_tmem_cols(FB, SPLIT) > 512 || NH < 64 || (FB & 7) ||
+            J.compound == 0) {
+            if (tid == 0) atomicAdd(prm.err_count, 1ull);
+            return;
+        }
+    }
+    if (tid == 0) {
+        for (int i = 0; i < TC_NS; ++i) {
+            mbar_init(&full_b[i], 1);
+            mbar_init(&full_a[i], 128);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&acc_full, 1);
+        mbar_init(&acc_empty, 128);
+        mbar_init(&fin, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        tmem_alloc(&tbase_s, 512);
+        tmem_relinquish();
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tb = tbase_s;
+    volatile int *abort = &abort_s;
+
+    const int64_t n_tiles = (int64_t)J.tiles_z * J.tiles_u * J.tiles_v;
+    const int n_steps = g.n_tx * g.n_ele;
+
+    if (warp == 4) {
+        // ---------------- producer: windows and TMA loads ----------------
+        uint32_t q = 0;
+        int last_q[TC_NS];
+#pragma unroll
+        for (int i = 0; i < TC_NS; ++i) last_q[i] = -1;
+        if (lane == 0) tma_prefetch_desc(&prm.tmap);
+        bool stop = false;   // warp-uniform
+        for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x) {
+            const int fb = (int)(item / n_tiles);
+            const int64_t tile = item % n_tiles;
+            const int tz = (int)(tile % J.tiles_z);
+            const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
+            const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+            for (int s0 = 0; s0 < n_steps && !stop; s0 += 32) {
+                const int s = s0 + lane;
+                int lo = 0, nk = 0;
+                bool act = false, ovf = false;
+                if (s < n_steps) {
+                    const int tx = s / g.n_ele, rx = s - tx * g.n_ele;
+                    act = tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf);
+                    if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
+                }
+                unsigned mask = __ballot_sync(0xffffffffu, act);
+                while (mask) {
+                    const int i = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const int lo_i = __shfl_sync(0xffffffffu, lo, i);
+                    const int nk_i = __shfl_sync(0xffffffffu, nk, i);
+                    int okw = 1;
+                    if (lane == 0) {
+                        const int st = (int)(q % TC_NS);
+                        okw = mbar_wait(&empty[st], ((q / TC_NS) & 1u) ^ 1u, abort) ? 1 : 0;
+                        if (okw) {
+                            info[st] = TcInfo{s0 + i, lo_i, nk_i, 0};
+                            mbar_arrive_expect_tx(&full_b[st], (uint32_t)(nk_i * NP * 2048));
+                            const int64_t row0 = ((int64_t)(s0 + i) * J.n_fb + fb) * prm.rows_per_slab + lo_i;
+                            uint8_t *dst = Bs + st * stage_bytes;
+                            for (int j = 0; j < nk_i; ++j)
+                                for (int p = 0; p < NP; ++p)
+                                    tma_load_2d(dst + p * TC_PANEL_BYTES + j * 2048, &prm.tmap, &full_b[st], 64 * p,
+                                                (int32_t)(row0 + 16 * j));
+                            last_q[st] = (int)q;
+                        }
+                    }
+                    okw = __shfl_sync(0xffffffffu, okw, 0);
+                    ++q;
+                    if (!okw) { stop = true; break; }
+                }
+            }
+            if (!stop) {   // end-of-item record
+                int okw = 1;
+                if (lane == 0) {
+                    const int st = (int)(q % TC_NS);
+                    okw = mbar_wait(&empty[st], ((q / TC_NS) & 1u) ^ 1u, abort) ? 1 : 0;
+                    if (okw) {
+                        info[st] = TcInfo{-1, 0, 0, 1};
+                        mbar_arrive(&full_b[st]);
+                        last_q[st] = -1;   // no copy in flight
+                    }
+                }
+                okw = __shfl_sync(0xffffffffu, okw, 0);
+                ++q;
+                if (!okw) stop = true;
+            }
+        }
+        if (lane == 0 && stop) {
+            // let the copies in flight land before the CTA's shared memory goes
+            for (int st = 0; st < TC_NS; ++st)
+                if (last_q[st] >= 0) {
+                    volatile int dummy = 0;
+                    mbar_wait(&full_b[st], ((uint32_t)last_q[st] / TC_NS) & 1u, &dummy, 100000000ull);
+                }
+        }
+    } else if (warp == 5) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            uint32_t q = 0, it = 0;
+            bool issued = false;
+            for (int64_t item = blockIdx.x; item < prm.n_items && !*abort; item += gridDim.x, ++it) {
+                bool first = true, dr = false, di = false;
+                for (;;) {
+                    const int st = (int)(q % TC_NS);
+                    const uint32_t ph = (q / TC_NS) & 1u;
+                    if (!mbar_wait(&full_b[st], ph, abort) || !mbar_wait(&full_a[st], ph, abort)) break;
+                    const TcInfo inf = read_info(&info[st]);
+                    ++q;
+                    if (inf.end) {
+                        umma_commit(&acc_full);
+                        mbar_arrive(&empty[st]);
+                        break;
+                    }
+                    if (first) {
+                        if (!mbar_wait(&acc_empty, (it & 1u) ^ 1u, abort)) break;
+                        first = false;
+                    }
+                    tmem_fence_after_sync();
+                    const uint32_t bbase = smem_u32(Bs + st * stage_bytes);
+                    const uint32_t acol = (uint32_t)(a_col0 + st * NMAT * 16);
+                    for (int j = 0; j < inf.nk; ++j) {
+                        const uint64_t bd = sdesc_mn_sw128(bbase + j * 2048, TC_PANEL_BYTES, 1024);
+#pragma unroll
+                        for (int mat = 0; mat < NMAT; ++mat) {
+                            const bool re = mat < NMAT / 2;
+                            const uint32_t d = tb + (re ? 0u : (uint32_t)N16);
+                            umma_f16_ts(d, tb + acol + mat * 16 + 8 * j, bd, idesc, (re ? dr : di) ? 1u : 0u);
+                            if (re) dr = true; else di = true;
+                        }
+                    }
+                    umma_commit(&empty[st]);
+                    issued = true;
+                }
+            }
+            if (*abort && issued) {   // the MMAs in flight complete before the columns are freed
+                umma_commit(&fin);
+                volatile int dummy = 0;
+                mbar_wait(&fin, 0, &dummy, 100000000ull);
+            }
+        }
+    } else {
+        // ---------------- weight builders + epilogue (warps 0-3) ----------------
+        const uint32_t lane_base = tb + ((uint32_t)(32 * warp) << 16);
+        const int m = tid;                  // voxel row of the tile = tensor-memory lane
+        const int lu = m % TC_TU, lv = m / TC_TU;
+        const int64_t n_rxkey = g.n_u * g.n_z, n_txkey = g.n_v * g.n_z;
+        uint32_t q = 0, it = 0;
+        for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x, ++it) {
+            const int fb = (int)(item / n_tiles);
+            const int64_t tile = item % n_tiles;
+            const int tz = (int)(tile % J.tiles_z);
+            const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
+            const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+            const int64_t iz = tz, iu = (int64_t)tu * TC_TU + lu, iv = (int64_t)tv * TC_TV + lv;
+            const bool valid = iz < g.n_z && iu < g.n_u && iv < g.n_v;
+            const int64_t rxkey = valid ? iu * g.n_z + iz : 0;
+            const int64_t txkey = valid ? iv * g.n_z + iz : 0;
+            int cur_tx = -1;
+            float itx = 0.f, ptr = 0.f, pti = 0.f;
+            bool cone = false, any = false;
+            int pre_s = -1;
+            float4 pre_e = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (;;) {
+                const int st = (int)(q % TC_NS);
+                if (!warp_wait(&full_b[st], (q / TC_NS) & 1u, abort)) break;
+                const TcInfo inf = read_info(&info[st]);
+                ++q;
+                if (inf.end) {
+                    mbar_arrive(&full_a[st]);
+                    break;
+                }
+                const int tx = inf.s / g.n_ele, rx = inf.s - tx * g.n_ele;
+                if (tx != cur_tx) {
+                    cur_tx = tx;
+                    const float4 t = valid ? __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey])
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                    itx = t.x; ptr = t.y; pti = t.z;
+                    cone = valid && t.w != 0.0f &&
+                           (g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0);
+                }
+                float4 e;
+                if (pre_s == inf.s) e = pre_e;
+                else e = valid ? __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                // the next step's receive entry, loaded while this one is built
+                if (valid && rx + 1 < g.n_ele) {
+                    pre_s = inf.s + 1;
+                    pre_e = __ldg(&g.rx_tab[(int64_t)(rx + 1) * n_rxkey + rxkey]);
+                } else {
+                    pre_s = -1;
+                }
+                const float ab = ab_value(g, tx, rx);
+                const float2 abp = ab_phasor(g, tx, rx);
+                const float idx = __fadd_rn(__fadd_rn(itx, e.x), ab);
+                const float fl = floorf(idx);
+                bool ok = cone && e.w > 0.0f && fl >= (float)KT::LO && fl < (float)(J.n_sample - 1 - KT::HI);
+                int o = ok ? (int)fl - KT::LO - inf.lo : 0;
+                if (ok && (o < 0 || o + TAPS > 16 * inf.nk)) {   // never expected: window bound violated
+                    atomicAdd(prm.err_count, 1ull);
+                    ok = false;
+                    o = 0;
+                }
+                float w[TAPS];
+                poly_weights<KIND, 6>(ok ? idx - fl : 0.0f, w);
+                // P = apod e^{j phi_tx} e^{j phi_rx} e^{j phi_ab} (apod folded in (ar, ai)), scaled
+                const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
+                const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
+                const float py = ok ? TC_SCALE * fmaf(qx, abp.y, qy * abp.x) : 0.0f;
+                tmem_fence_after_sync();
+                const uint32_t acol = lane_base + (uint32_t)(a_col0 + st * NMAT * 16);
+                auto emit_chunks = [&](const float *v, int nchunk) {
+                    for (int j = 0; j < nchunk; ++j) {
+                        uint32_t rh[8], ih[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {
+                            const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
+                            rh[c] = tc_pack(a * px, b * px);
+                            ih[c] = tc_pack(a * py, b * py);
+                        }
+                        if constexpr (SPLIT) {
+                            uint32_t rl[8], il[8];
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) {
+                                const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
+                                rl[c] = tc_pack_rem(a * px, b * px, rh[c]);
+                                il[c] = tc_pack_rem(a * py, b * py, ih[c]);
+                            }
+                            tmem_st8(acol + 0 * 16 + 8 * j, rh);
+                            tmem_st8(acol + 1 * 16 + 8 * j, rl);
+                            tmem_st8(acol + 2 * 16 + 8 * j, ih);
+                            tmem_st8(acol + 3 * 16 + 8 * j, il);
+                        } else {
+                            tmem_st8(acol + 0 * 16 + 8 * j, rh);
+                            tmem_st8(acol + 1 * 16 + 8 * j, ih);
+                        }
+                    }
+                };
+                if (inf.nk == 1) {
+                    float v[16];
+                    tc_place<TAPS, 16>(w, o, v);
+                    emit_chunks(v, 1);
+                } else {
+                    float v[32];
+                    tc_place<TAPS, 32>(w, o, v);
+                    emit_chunks(v, 2);
+                }
+                tmem_wait_st();
+                tmem_fence_before_sync();
+                mbar_arrive(&full_a[st]);
+                any = true;
+            }
+            if (__any_sync(0xffffffffu, *abort != 0)) break;
+            // ---- epilogue: D_r, D_i -> out (frames of this block) ----
+            if (!warp_wait(&acc_full, it & 1u, abort)) break;
+            tmem_fence_after_sync();
+            const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
+            for (int c = 0; c < N16; c += 16) {
+                uint32_t r[16], i16[16];
+                tmem_ld16(lane_base + (uint32_t)c, r);
+                tmem_ld16(lane_base + (uint32_t)(N16 + c), i16);
+                tmem_wait_ld16(r);
+                tmem_wait_ld16(i16);
+                if (valid) {
+#pragma unroll
+                    for (int h = 0; h < 8; ++h) {
+                        const int f = fb * FB + c / 2 + h;
+                        if (c / 2 + h < FB && f < J.n_frame) {
+                            float2 val = make_float2(0.f, 0.f);
+                            if (any) {
+                                val.x = (__uint_as_float(r[2 * h]) - __uint_as_float(i16[2 * h + 1])) * (1.0f / TC_SCALE);
+                                val.y = (__uint_as_float(r[2 * h + 1]) + __uint_as_float(i16[2 * h])) * (1.0f / TC_SCALE);
+                            }
+                            float2 *op = J.out + (int64_t)f * g.n_pix + pix;
+                            if (J.accumulate) { float2 x = *op; x.x += val.x; x.y += val.y; *op = x; }
+                            else *op = val;
+                        }
+                    }
+                }
+            }
+            tmem_fence_before_sync();
+            mbar_arrive(&acc_empty);
+        }
+    }
+    if (tid == 0 && *abort) atomicAdd(prm.err_count, 1ull);
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after_sync();
+        tmem_dealloc(tb, 512);
+    }
+}
+
+}  // namespace rcabf

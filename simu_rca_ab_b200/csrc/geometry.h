@@ -30,6 +30,7 @@ struct TuneChoice {
     int vb = 0;
     int fb = 0;
     TileShape ts{0, 0, 0};
+    int tc = 0;       // tensor-core kernel: 1 single FP16 weights, 2 hi + remainder weights
 };
 
 // Spread of the table delay inside the tiles of one shape, used to size the

@@ -15,6 +15,7 @@ struct IngestParams {
     int32_t fb, n_fb;
     void *S;
     int64_t slab_bytes;
+    int32_t n_rows;        // rows written per slab: n_sample, or more with zero rows past the record
 };
 
 struct RangeParams {
@@ -68,6 +69,16 @@ cudaError_t launch_fused_vb(int kind, int d, int tm, int fb, int store, const Fu
                             size_t smem, cudaStream_t st);
 cudaError_t prepare_fused_vb(int kind, int d, int tm, int fb, int store, size_t smem);
 int fused_vb_occupancy(int kind, int d, int tm, int fb, int store, size_t smem);
+
+// Tensor-core kernel (FP16 slabs, EXACT tables, compounded output; one CTA
+// per SM, all 512 tensor-memory columns): fb frames per block (multiple of
+// 8, 32..tc_max_frames_per_block(split)), slabs of rows_per_slab rows of
+// 2 fb halfs.  split = 1: weights as two FP16 terms (hi + remainder).
+cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, int rows_per_slab, int64_t n_items,
+                            unsigned long long *err, int n_sm, cudaStream_t st);
+int tc_max_frames_per_block(int split);
+int tc_tmem_columns(int fb, int split);
+size_t tc_launch_smem(int fb);
 
 // Plain kernel: one frame.
 cudaError_t launch_plain(int mode, int kind, const PlainParams &p, cudaStream_t st);

@@ -189,7 +189,8 @@ class Acquisition:
 
 _STORAGE = {"float32": 0, "single": 0, "fp32": 0, "float16": 1, "half": 1, "fp16": 1,
             "bfloat16": 2, "bf16": 2}
-_KERNEL = {"auto": 0, "fused": 1, "plain": 2, "fused_noblock": 3, "fused_tmem": 4, "fused_regs": 5}
+_KERNEL = {"auto": 0, "fused": 1, "plain": 2, "fused_noblock": 3, "fused_tmem": 4, "fused_regs": 5,
+           "fused_tc": 6, "fused_tc_fp16w": 7}
 _TABLES = {"exact": 0, "ref_compat": 1}
 
 

@@ -5,7 +5,10 @@
   contraction (oracle/_ref/librca_ref_gpu_strict.so), tolerance 1e-4
   relative RMS (expected: identical bits).
 * EXACT tables: against the FP64 oracle, tolerance -60 dB RMS for FP32 and
-  FP16 storage (BF16 storage: -45 dB, its 8-bit mantissa).
+  FP16 storage.  BF16 storage cannot reach -60 dB: rounding the channel data
+  to an 8-bit mantissa alone costs about -57 dB.  For it the bar is that the
+  kernel adds nothing to that rounding: -60 dB against the FP64 oracle run on
+  the BF16-rounded data, and the total within 1 dB of that storage floor.
 * Internal consistency: fused vs plain kernel, frame-block sizes, batch vs
   single launches, per-transmit vs compounded, both receive orientations,
   point-list grids, the transmit-cone mask, real (interleaved RF) input.
@@ -23,7 +26,29 @@ pytestmark = pytest.mark.gpu
 REF_TOL = 1e-4          # relative RMS, REF_COMPAT vs reference kernel
 DB_FP32 = -60.0         # dB RMS vs FP64 oracle
 DB_FP16 = -60.0
-DB_BF16 = -45.0
+DB_BF16 = None          # BF16: measured against its storage floor, see _check_bf16
+
+
+def _bf16_rounded(a):
+    """The channel data as BF16 storage holds it (round to nearest even)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a).astype(np.complex64))
+    r = torch.view_as_real(t).to(torch.bfloat16).to(torch.float32)
+    return torch.view_as_complex(r.contiguous()).numpy()
+
+
+def _check_bf16(out, ref, ref_rounded, label):
+    """BF16 storage: the kernel's error against the FP64 oracle of the
+    BF16-rounded data must be below -60 dB (the kernel adds nothing to the
+    storage rounding), and its total error within 1 dB of the storage floor
+    (the FP64 oracle of the rounded data against that of the original)."""
+    floor, _ = H.error_db(ref_rounded, ref)
+    own, _ = H.error_db(out, ref_rounded)
+    total, peak = H.error_db(out, ref)
+    print(f"{label} bfloat16: {total:.1f} dB RMS ({peak:.1f} dB peak) vs FP64; BF16 storage floor {floor:.1f} dB; "
+          f"kernel vs FP64 of the rounded data {own:.1f} dB")
+    assert own <= -60.0
+    assert total <= floor + 1.0
 
 
 @pytest.fixture(scope="module")
@@ -122,10 +147,16 @@ def test_exact_vs_fp64_oracle(bf, c0_small, interp, a, code, storage, tol):
     c64, cm64 = H.compound(f64, m64, True)
     ref, mref = H.matlab_shape(r, c64, cm64)
     db, mk = run(bf, data, G, T, P, O, interpolation=interp, lanczosOrder=max(a, 2), storage=storage)
+    assert np.allclose(mk, mref, rtol=1e-5, atol=1e-4)
+    if storage == "bfloat16":
+        dr = _bf16_rounded(np.asarray(data).transpose(3, 2, 1, 0).reshape(r.n_frame, r.n_tx, r.n_ch, r.n_sample))
+        f64r, m64r = H.run_fp64(r, code, a, data=dr)
+        refr, _ = H.matlab_shape(r, *H.compound(f64r, m64r, True))
+        _check_bf16(db, ref, refr, f"EXACT {interp}{a or ''}")
+        return
     rms, peak = H.error_db(db, ref)
     print(f"EXACT {interp}{a or ''} {storage}: {rms:.1f} dB RMS, {peak:.1f} dB peak vs FP64")
     assert rms <= tol
-    assert np.allclose(mk, mref, rtol=1e-5, atol=1e-4)
 
 
 def test_exact_receive_y_points_and_mask(bf):
@@ -271,9 +302,13 @@ def test_voxel_blocked_kernel_vs_fp64_on_c2_geometry(bf, c2_small, storage, tol)
     r = H.prepare(W.as_matlab(dn), g0.Geometry, g0.Transmit, w.Param, {"flagMaskTransmit": False})
     f64, m64 = H.run_fp64(r, H.INTERP_LANCZOS, 4, data=dn, pix=pix)
     c64, _ = H.compound(f64, m64, True)
-    rms, peak = H.error_db(out[:, pix], c64[:, 0])
-    print(f"voxel-blocked {storage} on c2 geometry: {rms:.1f} dB RMS, {peak:.1f} dB peak; plan {plan}")
-    assert rms <= tol
+    if storage == "bfloat16":
+        f64r, m64r = H.run_fp64(r, H.INTERP_LANCZOS, 4, data=_bf16_rounded(dn), pix=pix)
+        _check_bf16(out[:, pix], c64[:, 0], H.compound(f64r, m64r, True)[0][:, 0], "voxel-blocked, c2 geometry,")
+    else:
+        rms, peak = H.error_db(out[:, pix], c64[:, 0])
+        print(f"voxel-blocked {storage} on c2 geometry: {rms:.1f} dB RMS, {peak:.1f} dB peak; plan {plan}")
+        assert rms <= tol
     if storage == "float32":
         ref, plan2 = _beamform_dev(bf, w, data, storage, "fused_noblock")
         assert plan2["kernel"] == "fused"

@@ -79,6 +79,30 @@ def test_noalloc_matches_beamform_on_two_calls_in_a_row(cuda, storage):
     assert n.value == 0
 
 
+def test_noalloc_call_leaves_device_free_memory_unchanged(cuda):
+    """After the first call on the device (which looks up the static array
+    and, with lazy module loading, loads the module that holds it), further
+    calls change nothing in the device's free memory: they allocate nothing."""
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c0", n_frame=4)
+    eng, geom = _geometry(w)
+    iq = W.channel_data(w, seed=23, device=cuda).contiguous().to(torch.complex32)
+    out = torch.empty((w.n_frame, 1, geom.n_pix), dtype=torch.complex64, device=cuda)
+    mask = torch.empty((1, geom.n_pix), dtype=torch.float32, device=cuda)
+    args = [_args(eng, geom, w, iq, out, mask, L.STORE_F16) for _ in range(4)]
+    L.check(_noalloc(geom, args[0]), "rcabf_beamform_noalloc (set-up call)")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for a in args[1:]:
+        L.check(_noalloc(geom, a), "rcabf_beamform_noalloc")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes across noalloc calls"
+    assert float(out.abs().max()) > 0.0
+
+
 def test_noalloc_rejects_plans_larger_than_the_static_workspace(cuda):
     import torch
     from simu_rca_ab_b200 import _lib as L
