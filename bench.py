@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--no-simulator", action="store_true", help="skip the simulator timing")
     ap.add_argument("--no-ulm", action="store_true", help="skip the ULM super-localisation timing")
     ap.add_argument("--serving-requests", type=int, default=48)
-    ap.add_argument("--serving-rate", type=float, default=6.0, help="c3 Poisson arrival rate (requests/s)")
+    ap.add_argument("--serving-rates", default="6,60", help="c3 Poisson arrival rates (requests/s), comma-separated")
+    ap.add_argument("--no-serving-plain", action="store_true", help="skip serving the stream on the plain kernel")
     ap.add_argument("--plain-frames", type=int, default=10)
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference kernel on the GPU")
     ap.add_argument("--ref-gpu-frames", type=int, default=20,
@@ -169,11 +170,14 @@ def cpu_baseline(w, data_np, frames: int, zrows: int, kind_pref="reference"):
                       f"{total_units:.3e} units in {total_s:.1f} s on {cores} threads"}
 
 
-def serving_leg(eng, dev, n_requests: int, rate_hz: float, seed: int = 3):
-    """c3: a Poisson stream of mixed requests through the serving loop
-    (rcabf_server_*), submitted in real time at their arrival times; the
-    same stream served one request at a time by the plain per-frame kernel
-    is timed on the device (per request) and queued in arrival order."""
+def serving_leg(eng, dev, n_requests: int, rates, seed: int = 3, plain: bool = True):
+    """c3: Poisson streams of mixed requests through the serving loop
+    (rcabf_server_*), submitted in real time at their arrival times, at each
+    arrival rate of ``rates`` (the lowest first); then the lowest-rate stream
+    served again through the same loop with every request on the plain
+    per-frame kernel (one request per launch, no fusion), for comparison.
+    The admission budget is the configuration's 150 GB of HBM when the
+    device has it free (with 8 GB kept back), else what is free."""
     import warnings
 
     import numpy as np
@@ -184,34 +188,36 @@ def serving_leg(eng, dev, n_requests: int, rate_hz: float, seed: int = 3):
     from simu_rca_ab_b200.params import normalize
     from simu_rca_ab_b200.server import Server
 
-    reqs = W.serving_mix(seed, n_requests, rate_hz)
-    # geometry tables per probe / transmit set / grid, channel data per probe /
-    # transmit set (frames sliced per request): resident before the stream starts
     geoms, data = {}, {}
-    maxf = {}
-    for r in reqs:
-        maxf[(r.probe, r.n_tx)] = max(maxf.get((r.probe, r.n_tx), 0), r.n_frame)
-    for (probe, ntx), nf in maxf.items():
-        w = W.c3_workload(probe, ntx, W.C3_GRIDS[0], nf)
-        data[(probe, ntx)] = W.channel_data(w, seed=seed + probe + ntx, device=dev)
-    items = []
-    for r in reqs:
-        w = W.c3_workload(r.probe, r.n_tx, r.grid, r.n_frame)
-        key = (r.probe, r.n_tx, r.grid)
-        if key not in geoms:
-            g = w.groups[0]
-            with warnings.catch_warnings():
-                warnings.simplefilter("ignore")
-                geoms[key] = eng.geometry(normalize(np.zeros(1, np.complex64), g.Geometry, g.Transmit, w.Param,
-                                                    w.Options))
-        iq = data[(r.probe, r.n_tx)][: r.n_frame].contiguous()
-        if r.storage == "float16":
-            iq = iq.to(torch.complex32)
-        out = torch.empty((r.n_frame, 1, geoms[key].n_pix), dtype=torch.complex64, device=dev)
-        items.append((r, geoms[key], iq, out, w.units()))
-    total_units = sum(x[4] for x in items)
-    free, _ = torch.cuda.mem_get_info(dev)
-    budget = int(min(150e9, 0.5 * free))
+
+    def stream(rate_hz):
+        reqs = W.serving_mix(seed, n_requests, rate_hz)
+        # geometry tables per probe / transmit set / grid, channel data per
+        # probe / transmit set (frames sliced per request): resident before
+        # the stream starts
+        maxf = {}
+        for r in reqs:
+            maxf[(r.probe, r.n_tx)] = max(maxf.get((r.probe, r.n_tx), 0), r.n_frame)
+        for (probe, ntx), nf in maxf.items():
+            if (probe, ntx) not in data or data[(probe, ntx)].shape[0] < nf:
+                w = W.c3_workload(probe, ntx, W.C3_GRIDS[0], nf)
+                data[(probe, ntx)] = W.channel_data(w, seed=seed + probe + ntx, device=dev)
+        items = []
+        for r in reqs:
+            w = W.c3_workload(r.probe, r.n_tx, r.grid, r.n_frame)
+            key = (r.probe, r.n_tx, r.grid)
+            if key not in geoms:
+                g = w.groups[0]
+                with warnings.catch_warnings():
+                    warnings.simplefilter("ignore")
+                    geoms[key] = eng.geometry(normalize(np.zeros(1, np.complex64), g.Geometry, g.Transmit, w.Param,
+                                                        w.Options))
+            iq = data[(r.probe, r.n_tx)][: r.n_frame].contiguous()
+            if r.storage == "float16":
+                iq = iq.to(torch.complex32)
+            out = torch.empty((r.n_frame, 1, geoms[key].n_pix), dtype=torch.complex64, device=dev)
+            items.append((r, geoms[key], iq, out, w.units()))
+        return items
 
     def args(r, g, iq, out, kernel):
         code = L.STORE_F16 if r.storage == "float16" else L.STORE_F32
@@ -219,59 +225,54 @@ def serving_leg(eng, dev, n_requests: int, rate_hz: float, seed: int = 3):
         return eng.make_args(g, iq, iq_dtype=iqd, n_sample=iq.shape[-1], n_frame=iq.shape[0], out=out, mask=None,
                              compound=True, storage=code, kernel=kernel)
 
-    # the first launch of each kernel variant sets its shared-memory limit
-    # inside the stream, as it would in a live service
-    srv = Server(eng, budget, n_streams=4, max_queue=4 * n_requests, max_batch=24)
-    tickets = []
-    t0 = time.perf_counter()
-    for r, g, iq, out, _ in items:
-        delay = r.arrival_s - (time.perf_counter() - t0)
-        if delay > 0:
-            time.sleep(delay)
-        tickets.append(srv.submit(g, args(r, g, iq, out, L.KERNEL_AUTO), keep=(iq, out)))
-    for t in tickets:
-        srv.wait(t, 600.0)
-    st = srv.stats()
-    srv.close()
-
-    # the plain per-frame kernel: device time per request (2 frames timed,
-    # scaled by frames: one launch per frame), then a FIFO queue on the arrivals
-    svc = []
-    for r, g, iq, out, _ in items:
-        k = min(2, r.n_frame)
-        a = args(r, g, iq[:k], out[:k], L.KERNEL_PLAIN)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        eng.run(g, a)
-        e1.record()
+    def serve(items, kernel, budget):
+        # the first launch of each kernel variant sets its shared-memory limit
+        # inside the stream, as it would in a live service
+        srv = Server(eng, budget, n_streams=4, max_queue=4 * n_requests, max_batch=24)
+        tickets = []
+        t0 = time.perf_counter()
+        for r, g, iq, out, _ in items:
+            delay = r.arrival_s - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(g, args(r, g, iq, out, kernel), keep=(iq, out)))
+        for t in tickets:
+            srv.wait(t, 900.0)
+        st = srv.stats()
+        srv.close()
         torch.cuda.synchronize()
-        svc.append(e0.elapsed_time(e1) * r.n_frame / k)
-    lat, free_at = [], 0.0
-    for (r, *_), s_ms in zip(items, svc):
-        start = max(r.arrival_s * 1e3, free_at)
-        free_at = start + s_ms
-        lat.append(free_at - r.arrival_s * 1e3)
-    lat_sorted = sorted(lat)
+        return {"p50_ms": st.p50_ms, "p95_ms": st.p95_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
+                "max_ms": st.max_ms, "value": st.units_done / st.span_s if st.span_s > 0 else None, "unit": UNIT,
+                "launches": st.launches, "requests": len(items), "busy_s": st.busy_s, "span_s": st.span_s,
+                "arena_peak_bytes": st.arena_peak_bytes}
 
-    def pct(v, q):
-        return float(np.percentile(np.asarray(v), q))
-
-    span_plain = (free_at - items[0][0].arrival_s * 1e3) * 1e-3
-    return {
-        "workload": f"c3 serving mix: {n_requests} requests, Poisson arrivals at {rate_hz:g}/s (seed {seed}); "
-                    "probe 64+64 or 128+128, 1-32 tx, 1-64 frames, grids 32x32x64..128x128x256, FP32/FP16 "
-                    "storage, f-number 1.5, Lanczos a=3; channel data and geometry tables resident",
-        "requests": n_requests, "units": total_units, "hbm_budget_bytes": budget,
-        "p50_ms": st.p50_ms, "p95_ms": st.p95_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
-        "value": st.units_done / st.span_s if st.span_s > 0 else None, "unit": UNIT,
-        "launches": st.launches, "busy_s": st.busy_s, "span_s": st.span_s,
-        "arena_peak_bytes": st.arena_peak_bytes,
-        "plain_kernel": {"p50_ms": pct(lat_sorted, 50), "p95_ms": pct(lat_sorted, 95), "p99_ms": pct(lat_sorted, 99),
-                         "value": total_units / span_plain, "unit": UNIT,
-                         "service_s": sum(svc) * 1e-3,
-                         "how": "plain_das_kernel per request (device time of 2 frames x frames/2), "
-                                "FIFO queue on the same arrival times"},
-    }
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(min(150e9, free - 8e9))
+    res = {"workload": f"c3 serving mix: {n_requests} requests per stream, Poisson arrivals (seed {seed}); probe "
+                       "64+64 or 128+128, 1-32 tx, 1-64 frames, grids 32x32x64..128x128x256, FP32/FP16 storage, "
+                       "f-number 1.5, Lanczos a=3; channel data and geometry tables resident",
+           "hbm_budget_bytes": budget,
+           "hbm_budget_note": "150 GB as configured" if budget >= 150e9 else
+                              f"150 GB configured; {free / 1e9:.1f} GB free on the device, 8 GB kept back",
+           "rates": []}
+    items0 = None
+    for rate in sorted(rates):
+        items = stream(rate)
+        if items0 is None:
+            items0 = items
+        r = serve(items, L.KERNEL_AUTO, budget)
+        r["rate_hz"] = rate
+        r["units"] = sum(x[4] for x in items)
+        r["fused_launches"] = r["launches"] < r["requests"]
+        res["rates"].append(r)
+    if plain and items0 is not None:
+        r = serve(items0, L.KERNEL_PLAIN, budget)
+        r["rate_hz"] = min(rates)
+        r["how"] = "the lowest-rate stream served through rcabf_server_* with every request on plain_das_kernel"
+        res["plain_kernel"] = r
+    return res
 
 
 def ulm_leg(dev, seed: int = 11, nz: int = 256, nx: int = 256, nt: int = 400, n_bubbles: int = 48):
@@ -700,7 +701,8 @@ def main():
     serving = None
     if not a.no_serving and rank == 0:
         try:
-            serving = serving_leg(eng, dev, a.serving_requests, a.serving_rate)
+            serving = serving_leg(eng, dev, a.serving_requests, [float(x) for x in a.serving_rates.split(",")],
+                                  plain=not a.no_serving_plain)
         except Exception as ex:   # reported, not hidden: the line says what failed
             serving = {"error": f"{type(ex).__name__}: {ex}"}
         torch.cuda.synchronize()

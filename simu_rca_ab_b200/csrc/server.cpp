@@ -155,7 +155,7 @@ static bool same_variant(const Request *a, const Request *b)
     return a->batchable && b->batchable && a->g->device == b->g->device && a->g->mode == b->g->mode && a->g->kind == b->g->kind &&
            a->a.storage == b->a.storage && a->plan.kernel == RCABF_KERNEL_FUSED &&
            b->plan.kernel == RCABF_KERNEL_FUSED && a->plan.fb == b->plan.fb && a->plan.vb == b->plan.vb &&
-           a->plan.d == b->plan.d;
+           a->plan.d == b->plan.d && a->plan.tc == b->plan.tc;
 }
 
 static void finish_locked(rcabf_server *s, Request *r, int status, Clock::time_point now)
@@ -376,7 +376,7 @@ int rcabf_server_submit(rcabf_server *s, const rcabf_geometry *g, const rcabf_be
         pinned.frames_per_block = r->plan.fb;
         Plan p2;
         if (plan_beamform(gg, &pinned, p2) == RCABF_OK && p2.vb == r->plan.vb && p2.d == r->plan.d &&
-            p2.fb == r->plan.fb && p2.total == r->plan.total) {
+            p2.tc == r->plan.tc && p2.fb == r->plan.fb && p2.total == r->plan.total) {
             r->a = pinned;
             r->batchable = true;
         }

@@ -1,0 +1,162 @@
+"""The tensor-core kernel (fused_tc_kernel.cuh, tcgen05.mma) through the C ABI:
+against the FP64 oracle (-60 dB RMS), against the voxel-blocked SIMT kernel on
+the same FP16 slabs, over both weight precisions (hi + remainder FP16 terms,
+single FP16), the interpolation kernels, frame blocks, partial tiles at the
+grid edges, accumulation into the output, and the cases it declines."""
+import ctypes as C
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import host as H
+
+pytestmark = pytest.mark.gpu
+
+DB_TOL = -60.0
+
+
+def _errcount():
+    from simu_rca_ab_b200 import _lib as L
+    n = C.c_int64()
+    L.check(L.lib().rcabf_take_error_count(C.byref(n)))
+    return n.value
+
+
+def _setup(w, seed):
+    import torch
+    from simu_rca_ab_b200 import beamformer as B
+    from simu_rca_ab_b200 import workloads as W
+    from simu_rca_ab_b200.params import normalize
+    g0 = w.groups[0]
+    data = W.channel_data(w, seed=seed, device="cuda")
+    eng = B.default_engine()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geom = eng.geometry(normalize(np.zeros(1, np.complex64), g0.Geometry, g0.Transmit, w.Param, w.Options))
+    return data, eng, geom, data.contiguous().to(torch.complex32)
+
+
+def _run(w, eng, geom, iq, kernel, compound=True, accumulate=False, out=None, storage=None):
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    if out is None:
+        out = torch.empty((w.n_frame, 1 if compound else geom.n_tx, geom.n_pix), dtype=torch.complex64,
+                          device="cuda")
+    a = eng.make_args(geom, iq, iq_dtype=L.IQ_C32 if iq.dtype == torch.complex32 else L.IQ_C64,
+                      n_sample=w.n_sample, n_frame=w.n_frame, out=out, mask=None, compound=compound,
+                      storage=L.STORE_F16 if storage is None else storage, kernel=kernel, accumulate=accumulate)
+    plan = eng.plan(geom, a)
+    eng.run(geom, a)
+    torch.cuda.synchronize()
+    return out, plan
+
+
+def _fp64(w, data, pix):
+    from simu_rca_ab_b200 import workloads as W
+    g0 = w.groups[0]
+    dn = data.cpu().numpy()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        r = H.prepare(W.as_matlab(dn), g0.Geometry, g0.Transmit, w.Param, {"flagMaskTransmit": False})
+    code = {"quadratic": H.INTERP_QUAD3, "ref6": H.INTERP_REF6}.get(w.Options.get("interpolation"), H.INTERP_LANCZOS)
+    f64, m64 = H.run_fp64(r, code, w.lanczos_a, data=dn, pix=pix)
+    return H.compound(f64, m64, True)[0][:, 0]
+
+
+@pytest.fixture(scope="module")
+def c2_40(cuda):
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c2", n_frame=40)
+    return (w,) + _setup(w, 5)
+
+
+@pytest.mark.parametrize("kname", ["tc", "tc16"])
+def test_tensor_core_kernel_vs_fp64_and_simt_on_the_ensemble_geometry(c2_40, kname):
+    from simu_rca_ab_b200 import _lib as L
+    w, data, eng, geom, iq = c2_40
+    kern = {"tc": L.KERNEL_FUSED_TC, "tc16": L.KERNEL_FUSED_TC_FP16W}[kname]
+    out, plan = _run(w, eng, geom, iq, kern)
+    assert plan["kernel"].startswith("fused_tensor_core"), plan
+    assert _errcount() == 0
+    ref_simt, plan_s = _run(w, eng, geom, iq, L.KERNEL_FUSED_TMEM)
+    assert plan_s["kernel"] == "fused_voxel_blocked_tmem"
+    o = out[:, 0].cpu().numpy()
+    pix = np.sort(np.random.default_rng(17).choice(geom.n_pix, 1024, replace=False))
+    rms, peak = H.error_db(o[:, pix], _fp64(w, data, pix))
+    rel = H.rel_rms(o, ref_simt[:, 0].cpu().numpy())
+    print(f"{kname} (c2 geometry, 40 frames, plan {plan}): {rms:.1f} dB RMS, {peak:.1f} dB peak vs FP64; "
+          f"rel RMS vs the SIMT kernel {rel:.2e}")
+    assert rms <= DB_TOL
+    # the SIMT kernel rounds nothing but the samples: the hi + remainder
+    # weights agree with it far below the storage error, single FP16 weights
+    # within their own rounding
+    assert rel < (2e-5 if kname == "tc" else 1e-3)
+    assert np.isfinite(o).all()
+
+
+@pytest.mark.parametrize("kname,n_frame", [("tc", 100), ("tc16", 100), ("tc", 33)])
+def test_frame_blocks_and_padding(cuda, kname, n_frame):
+    """Several frame blocks (100 frames: two blocks of 56 hi + remainder, one of
+    104 single) and a block padded from 33 to 40 frames give every frame the
+    SIMT kernel's value."""
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c2", n_frame=n_frame, grid_scale=0.5)
+    data, eng, geom, iq = _setup(w, 8)
+    kern = {"tc": L.KERNEL_FUSED_TC, "tc16": L.KERNEL_FUSED_TC_FP16W}[kname]
+    out, plan = _run(w, eng, geom, iq, kern)
+    ref, _ = _run(w, eng, geom, iq, L.KERNEL_FUSED_TMEM)
+    print(kname, n_frame, plan)
+    assert _errcount() == 0
+    rel = H.rel_rms(out.cpu().numpy(), ref.cpu().numpy())
+    assert rel < (2e-5 if kname == "tc" else 1e-3), rel
+    # every frame carries signal (no frame of a block left out)
+    per_frame = out[:, 0].abs().amax(dim=1).cpu().numpy()
+    assert (per_frame > 0).all()
+
+
+@pytest.mark.parametrize("interp,a", [("quadratic", 0), ("ref6", 0), ("lanczos", 2), ("lanczos", 3)])
+def test_interpolation_kernels_and_partial_tiles(cuda, interp, a):
+    """Every interpolation kernel, on a 48 x 48 x 96 grid (partial tiles along
+    both lateral axes), against the FP64 oracle."""
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import workloads as W
+    w = W.get("c0", n_frame=32, grid_scale=0.75)
+    w.Options = {**w.Options, "interpolation": interp, "lanczosOrder": max(a, 2)}
+    if a:
+        w.lanczos_a = a
+    data, eng, geom, iq = _setup(w, 9)
+    out, plan = _run(w, eng, geom, iq, L.KERNEL_FUSED_TC)
+    assert plan["kernel"] == "fused_tensor_core", plan
+    assert _errcount() == 0
+    o = out[:, 0].cpu().numpy()
+    pix = np.sort(np.random.default_rng(19).choice(geom.n_pix, 1024, replace=False))
+    rms, _ = H.error_db(o[:, pix], _fp64(w, data, pix))
+    print(f"tensor-core {interp}{a or ''} on a 48x48x96 grid: {rms:.1f} dB vs FP64")
+    assert rms <= DB_TOL
+
+
+def test_accumulate_adds_into_the_output(c2_40):
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    w, data, eng, geom, iq = c2_40
+    once, _ = _run(w, eng, geom, iq, L.KERNEL_FUSED_TC)
+    twice, _ = _run(w, eng, geom, iq, L.KERNEL_FUSED_TC)
+    _run(w, eng, geom, iq, L.KERNEL_FUSED_TC, accumulate=True, out=twice)
+    assert torch.equal(twice, 2 * once)
+
+
+def test_declined_cases(c2_40):
+    """Per-transmit output, FP32 storage and fewer than 32 frames are not
+    tensor-core work: the call is refused (RCABF_ERR_UNSUPPORTED)."""
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import workloads as W
+    w, data, eng, geom, iq = c2_40
+    with pytest.raises(Exception):
+        _run(w, eng, geom, iq, L.KERNEL_FUSED_TC, compound=False)
+    with pytest.raises(Exception):
+        _run(w, eng, geom, data.contiguous(), L.KERNEL_FUSED_TC, storage=L.STORE_F32)
+    w8 = W.get("c2", n_frame=8)
+    with pytest.raises(Exception):
+        _run(w8, eng, geom, iq[:8].contiguous(), L.KERNEL_FUSED_TC)
