@@ -312,10 +312,14 @@ typedef struct rcabf_tune_result {
     int32_t window_rows;          /* sample rows staged per step (the shared-memory window depth) */
     int32_t candidates;           /* launch choices timed */
     double best_ms, default_ms;   /* per call: the chosen one, the planner's own */
+    int32_t tensor_core;          /* 1: the choice is the tensor-core kernel (RCABF_KERNEL_FUSED_TC) */
+    int32_t reserved;
 } rcabf_tune_result;
 
 /* Times the fused kernel's launch choices (tile shape, hence window depth,
- * frame block, kernel family) on these arguments and keeps the fastest for
+ * frame block, kernel family -- the tensor-core kernel with hi + remainder
+ * weights included where it applies; never the single-FP16-weight variant,
+ * which is chosen by name only) on these arguments and keeps the fastest for
  * this geometry, frame count and storage: later calls with
  * frames_per_block = 0 (or the chosen block) plan with it.  No counterpart
  * in the reference, whose launch shape is fixed (RCA.m:640-650).

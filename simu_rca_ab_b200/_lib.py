@@ -74,6 +74,7 @@ class TuneResult(C.Structure):
         ("tile_u", C.c_int32), ("tile_v", C.c_int32), ("tile_z", C.c_int32),
         ("window_rows", C.c_int32), ("candidates", C.c_int32),
         ("best_ms", C.c_double), ("default_ms", C.c_double),
+        ("tensor_core", C.c_int32), ("reserved", C.c_int32),
     ]
 
 

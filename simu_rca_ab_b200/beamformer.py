@@ -231,7 +231,7 @@ class Engine:
         with torch.cuda.device(self.device):
             L.check(L.lib().rcabf_autotune(C.c_void_p(geom.ptr), C.byref(a), C.c_void_p(_stream_ptr(stream)),
                                            iters, C.byref(r)), "rcabf_autotune")
-        return {f: getattr(r, f) for f, _ in L.TuneResult._fields_ if f != "struct_size"}
+        return {f: getattr(r, f) for f, _ in L.TuneResult._fields_ if f not in ("struct_size", "reserved")}
 
     def workspace_bytes(self, geom: GeometryHandle, a: L.BeamformArgs) -> int:
         n = C.c_size_t()

@@ -940,14 +940,18 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
 
     double default_ms = 0.0;
     s = time_plan(p0, default_ms);
-    TuneChoice best{p0.vb, p0.fb, p0.ts};
+    TuneChoice best{p0.vb, p0.fb, p0.ts, p0.tc};
     double best_ms = default_ms;
     auto consider = [&](const TuneChoice &c) {
         Plan p;
         if (plan_beamform(g, &b, p, &c) != RCABF_OK) return;   // does not fit
         double ms = 0.0;
         if (time_plan(p, ms) != RCABF_OK) { cudaGetLastError(); return; }
-        if (ms < best_ms) { best_ms = ms; best = c; }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+            best.fb = p.fb;   // the frame block the choice planned (the tensor-core kernel picks its own)
+        }
     };
     if (s == RCABF_OK) {
         if (p0.vb) {
@@ -970,6 +974,13 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
                 if (fb > 2 * a->n_frame) continue;
                 consider(TuneChoice{p0.vb == 2 ? 1 : 2, fb, bt});
             }
+        }
+        // the tensor-core kernel (hi + remainder weights) where it applies
+        if (!p0.tc) {
+            TuneChoice tcc;
+            tcc.tc = 2;
+            tcc.ts = TileShape{TC_TILE_U, TC_TILE_V, 1};
+            consider(tcc);
         }
         // the one-voxel-per-thread kernel at its own frame blocks
         rcabf_beamform_args nb = b;
@@ -1002,6 +1013,7 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
     res->candidates = tried;
     res->best_ms = best_ms;
     res->default_ms = default_ms;
+    res->tensor_core = pb.tc ? 1 : 0;
     return RCABF_OK;
 }
 

@@ -22,21 +22,27 @@
 // FP16 rounding (~11 bits).  All weights are scaled by 2^8 (undone in the
 // epilogue) so that the remainder terms stay out of the FP16 subnormal range.
 //
-// Roles (192 threads): warps 0-3 build the weight matrices, one voxel per
-// thread, straight into tensor memory (lane = voxel row; tcgen05.st), and
-// write the outputs; warp 4 computes the windows of 32 steps at a time and
-// loads each active step's window with 2-D TMA (128-byte swizzle) into a
-// ring of NS shared-memory stages; warp 5 issues the MMAs (A from tensor
-// memory, B from shared memory) and commits them to the stage's "empty"
-// barrier.  Steps whose window is empty for the whole tile are skipped by
-// every role alike: the producer passes each active step's record (step,
-// window start, 16-row chunks) through the stage ring, followed by an
-// end-of-item record.  Every wait is bounded (mbar_wait): a wait that runs
-// out sets an abort flag, counts an error and every role leaves its loop.
+// Roles (320 threads): two groups of four warps build the weight matrices,
+// one voxel per thread, straight into tensor memory (lane = voxel row;
+// tcgen05.st), alternating records (group 0 the even ones, group 1 the odd
+// ones, so that one group's setup overlaps the other's), and the group that
+// meets an item's end record writes that item's outputs; warp 8 computes
+// the windows of 32 steps at a time and loads each active step's window with
+// 2-D TMA (128-byte swizzle) into a ring of TC_NSB shared-memory stages, up
+// to TC_NSB records ahead of the MMAs, so the load latency stays off the
+// critical path; warp 9 issues the MMAs (A from one of TC_NSA tensor-memory
+// weight slots, B from shared memory) and commits them to the slot's and
+// the stage's "empty" barriers.  Steps whose window is empty for the whole
+// tile are skipped by every role alike: the producer passes each active
+// step's record (step, window start, 16-row chunks, item) through the stage
+// ring, then an end-of-item record (with the item's count of active steps),
+// and after the last item one final record per builder group.  Every wait
+// is bounded (mbar_wait): a wait that runs out sets an abort flag, counts an
+// error and every role leaves its loop.
 //
 // Tensor memory (512 columns, one CTA per SM): D_r at column 0, D_i at
-// column N16, then NS stages of NMAT weight matrices of 16 columns (32 FP16
-// per row: K <= 32).
+// column N16, then TC_NSA slots of NMAT weight matrices of 16 columns (32
+// FP16 per row: K <= 32).
 #pragma once
 
 #include <cuda.h>
@@ -47,22 +53,25 @@
 
 namespace rcabf {
 
-constexpr int TC_THREADS = 192;
+constexpr int TC_GROUPS = 2;               // builder groups of 4 warps
+constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
+constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_TU = TC_TILE_U, TC_TV = TC_TILE_V;   // tile: TU (receive axis) x TV (steering axis) x 1 depth
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
 static_assert(TC_TU * TC_TV == 128, "one voxel per tensor-memory lane");
-constexpr int TC_NS = 3;                   // pipeline stages
+constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
+constexpr int TC_NSB = 12;                 // window stages in shared memory
 constexpr int TC_PANEL_BYTES = TC_KCH * 2048;   // one 64-element panel of B: TC_KCH x (16 rows x 128 B)
 constexpr float TC_SCALE = 256.0f;
 constexpr RCABF_HD int tc_nmat(bool split) { return split ? 4 : 2; }
 constexpr RCABF_HD int tc_n16(int fb) { return (2 * fb + 15) / 16 * 16; }
 constexpr RCABF_HD int tc_panels(int fb) { return (2 * fb + 63) / 64; }
 // tensor-memory columns the kernel needs at frame block fb
-constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return 2 * tc_n16(fb) + TC_NS * (split ? 4 : 2) * 16; }
+constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return 2 * tc_n16(fb) + TC_NSA * (split ? 4 : 2) * 16; }
 // largest frame block that fits the 512 columns
 constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 80 : 104; }
-// dynamic shared memory: NS stages of B panels + 1 KB for the 1024-byte alignment
-constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NS * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+// dynamic shared memory: TC_NSB stages of B panels + 1 KB for the 1024-byte alignment
+constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
 
 // All lanes wait on the barrier; the warp proceeds (converged) only if every
 // lane saw the phase complete.
@@ -72,15 +81,19 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volati
     return __all_sync(0xffffffffu, ok);
 }
 
+// One record of the stage ring.  kind: TC_STEP (an active step: s, window
+// start lo, nk 16-row chunks), TC_END (end of item `it`, n active steps),
+// TC_FINAL (no more items).  it counts the CTA's items.
+enum TcKind : int32_t { TC_STEP = 0, TC_END = 1, TC_FINAL = 2 };
 struct TcInfo {
-    int32_t s, lo, nk, end;
+    int32_t kind, s, lo, nk, it, n;
 };
 // a record written by another thread (published through an mbarrier)
 __device__ __forceinline__ TcInfo read_info(const TcInfo *p)
 {
     const volatile TcInfo *v = p;
     TcInfo r;
-    r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.end = v->end;
+    r.kind = v->kind; r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.it = v->it; r.n = v->n;
     return r;
 }
 
@@ -168,9 +181,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
 
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full_b[TC_NS], full_a[TC_NS], empty[TC_NS];
+    __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], empty_a[TC_NSA];
     __shared__ uint64_t acc_full, acc_empty, fin;
-    __shared__ TcInfo info[TC_NS];
+    __shared__ TcInfo info[TC_NSB];
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
     uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -186,10 +199,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         }
     }
     if (tid == 0) {
-        for (int i = 0; i < TC_NS; ++i) {
+        for (int i = 0; i < TC_NSB; ++i) {
             mbar_init(&full_b[i], 1);
+            mbar_init(&empty_b[i], 1);
+        }
+        for (int i = 0; i < TC_NSA; ++i) {
             mbar_init(&full_a[i], 128);
-            mbar_init(&empty[i], 1);
+            mbar_init(&empty_a[i], 1);
         }
         mbar_init(&acc_full, 1);
         mbar_init(&acc_empty, 128);
@@ -210,20 +226,48 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const int64_t n_tiles = (int64_t)J.tiles_z * J.tiles_u * J.tiles_v;
     const int n_steps = g.n_tx * g.n_ele;
 
-    if (warp == 4) {
+    if (warp == TC_PRODUCER_WARP) {
         // ---------------- producer: windows and TMA loads ----------------
         uint32_t q = 0;
-        int last_q[TC_NS];
+        int last_q[TC_NSB];
 #pragma unroll
-        for (int i = 0; i < TC_NS; ++i) last_q[i] = -1;
+        for (int i = 0; i < TC_NSB; ++i) last_q[i] = -1;
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
         bool stop = false;   // warp-uniform
-        for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x) {
+        // one record into the ring (lane 0 writes; the warp learns whether it could)
+        auto emit = [&](const TcInfo rec, int64_t row0) {
+            int okw = 1;
+            if (lane == 0) {
+                const int st = (int)(q % TC_NSB);
+                okw = mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort) ? 1 : 0;
+                if (okw) {
+                    info[st] = rec;
+                    if (rec.kind == TC_STEP) {
+                        mbar_arrive_expect_tx(&full_b[st], (uint32_t)(rec.nk * NP * 2048));
+                        uint8_t *dst = Bs + st * stage_bytes;
+                        for (int j = 0; j < rec.nk; ++j)
+                            for (int p = 0; p < NP; ++p)
+                                tma_load_2d(dst + p * TC_PANEL_BYTES + j * 2048, &prm.tmap, &full_b[st], 64 * p,
+                                            (int32_t)(row0 + 16 * j));
+                        last_q[st] = (int)q;
+                    } else {
+                        mbar_arrive(&full_b[st]);
+                        last_q[st] = -1;   // no copy in flight
+                    }
+                }
+            }
+            okw = __shfl_sync(0xffffffffu, okw, 0);
+            ++q;
+            if (!okw) stop = true;
+        };
+        int it = 0;
+        for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x, ++it) {
             const int fb = (int)(item / n_tiles);
             const int64_t tile = item % n_tiles;
             const int tz = (int)(tile % J.tiles_z);
             const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
             const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+            int n_active = 0;
             for (int s0 = 0; s0 < n_steps && !stop; s0 += 32) {
                 const int s = s0 + lane;
                 int lo = 0, nk = 0;
@@ -234,94 +278,71 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
                 }
                 unsigned mask = __ballot_sync(0xffffffffu, act);
-                while (mask) {
+                while (mask && !stop) {
                     const int i = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const int lo_i = __shfl_sync(0xffffffffu, lo, i);
                     const int nk_i = __shfl_sync(0xffffffffu, nk, i);
-                    int okw = 1;
-                    if (lane == 0) {
-                        const int st = (int)(q % TC_NS);
-                        okw = mbar_wait(&empty[st], ((q / TC_NS) & 1u) ^ 1u, abort) ? 1 : 0;
-                        if (okw) {
-                            info[st] = TcInfo{s0 + i, lo_i, nk_i, 0};
-                            mbar_arrive_expect_tx(&full_b[st], (uint32_t)(nk_i * NP * 2048));
-                            const int64_t row0 = ((int64_t)(s0 + i) * J.n_fb + fb) * prm.rows_per_slab + lo_i;
-                            uint8_t *dst = Bs + st * stage_bytes;
-                            for (int j = 0; j < nk_i; ++j)
-                                for (int p = 0; p < NP; ++p)
-                                    tma_load_2d(dst + p * TC_PANEL_BYTES + j * 2048, &prm.tmap, &full_b[st], 64 * p,
-                                                (int32_t)(row0 + 16 * j));
-                            last_q[st] = (int)q;
-                        }
-                    }
-                    okw = __shfl_sync(0xffffffffu, okw, 0);
-                    ++q;
-                    if (!okw) { stop = true; break; }
+                    const int64_t row0 = ((int64_t)(s0 + i) * J.n_fb + fb) * prm.rows_per_slab + lo_i;
+                    emit(TcInfo{TC_STEP, s0 + i, lo_i, nk_i, it, 0}, row0);
+                    ++n_active;
                 }
             }
-            if (!stop) {   // end-of-item record
-                int okw = 1;
-                if (lane == 0) {
-                    const int st = (int)(q % TC_NS);
-                    okw = mbar_wait(&empty[st], ((q / TC_NS) & 1u) ^ 1u, abort) ? 1 : 0;
-                    if (okw) {
-                        info[st] = TcInfo{-1, 0, 0, 1};
-                        mbar_arrive(&full_b[st]);
-                        last_q[st] = -1;   // no copy in flight
-                    }
-                }
-                okw = __shfl_sync(0xffffffffu, okw, 0);
-                ++q;
-                if (!okw) stop = true;
-            }
+            if (!stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active}, 0);
         }
+        for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0}, 0);
         if (lane == 0 && stop) {
             // let the copies in flight land before the CTA's shared memory goes
-            for (int st = 0; st < TC_NS; ++st)
+            for (int st = 0; st < TC_NSB; ++st)
                 if (last_q[st] >= 0) {
                     volatile int dummy = 0;
-                    mbar_wait(&full_b[st], ((uint32_t)last_q[st] / TC_NS) & 1u, &dummy, 100000000ull);
+                    mbar_wait(&full_b[st], ((uint32_t)last_q[st] / TC_NSB) & 1u, &dummy, 100000000ull);
                 }
         }
-    } else if (warp == 5) {
+    } else if (warp == TC_MMA_WARP) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            uint32_t q = 0, it = 0;
-            bool issued = false;
-            for (int64_t item = blockIdx.x; item < prm.n_items && !*abort; item += gridDim.x, ++it) {
-                bool first = true, dr = false, di = false;
-                for (;;) {
-                    const int st = (int)(q % TC_NS);
-                    const uint32_t ph = (q / TC_NS) & 1u;
-                    if (!mbar_wait(&full_b[st], ph, abort) || !mbar_wait(&full_a[st], ph, abort)) break;
-                    const TcInfo inf = read_info(&info[st]);
-                    ++q;
-                    if (inf.end) {
-                        umma_commit(&acc_full);
-                        mbar_arrive(&empty[st]);
-                        break;
-                    }
-                    if (first) {
-                        if (!mbar_wait(&acc_empty, (it & 1u) ^ 1u, abort)) break;
-                        first = false;
-                    }
-                    tmem_fence_after_sync();
-                    const uint32_t bbase = smem_u32(Bs + st * stage_bytes);
-                    const uint32_t acol = (uint32_t)(a_col0 + st * NMAT * 16);
-                    for (int j = 0; j < inf.nk; ++j) {
-                        const uint64_t bd = sdesc_mn_sw128(bbase + j * 2048, TC_PANEL_BYTES, 1024);
-#pragma unroll
-                        for (int mat = 0; mat < NMAT; ++mat) {
-                            const bool re = mat < NMAT / 2;
-                            const uint32_t d = tb + (re ? 0u : (uint32_t)N16);
-                            umma_f16_ts(d, tb + acol + mat * 16 + 8 * j, bd, idesc, (re ? dr : di) ? 1u : 0u);
-                            if (re) dr = true; else di = true;
-                        }
-                    }
-                    umma_commit(&empty[st]);
-                    issued = true;
+            uint32_t q = 0;
+            bool issued = false, first = true, dr = false, di = false;
+            for (;;) {
+                const int bst = (int)(q % TC_NSB);
+                if (!mbar_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
+                const TcInfo inf = read_info(&info[bst]);
+                if (inf.kind == TC_FINAL) break;
+                const int ast = (int)(q % TC_NSA);
+                if (!mbar_wait(&full_a[ast], (q / TC_NSA) & 1u, abort)) break;
+                ++q;
+                // at an item's first record (its end record when no step is
+                // active): the previous item's outputs have been read out, so
+                // the accumulators may be overwritten or reported complete
+                if (first) {
+                    if (!mbar_wait(&acc_empty, ((uint32_t)inf.it & 1u) ^ 1u, abort)) break;
+                    first = false;
                 }
+                if (inf.kind == TC_END) {
+                    umma_commit(&acc_full);
+                    mbar_arrive(&empty_a[ast]);
+                    mbar_arrive(&empty_b[bst]);
+                    first = true;
+                    dr = di = false;
+                    continue;
+                }
+                tmem_fence_after_sync();
+                const uint32_t bbase = smem_u32(Bs + bst * stage_bytes);
+                const uint32_t acol = (uint32_t)(a_col0 + ast * NMAT * 16);
+                for (int j = 0; j < inf.nk; ++j) {
+                    const uint64_t bd = sdesc_mn_sw128(bbase + j * 2048, TC_PANEL_BYTES, 1024);
+#pragma unroll
+                    for (int mat = 0; mat < NMAT; ++mat) {
+                        const bool re = mat < NMAT / 2;
+                        const uint32_t d = tb + (re ? 0u : (uint32_t)N16);
+                        umma_f16_ts(d, tb + acol + mat * 16 + 8 * j, bd, idesc, (re ? dr : di) ? 1u : 0u);
+                        if (re) dr = true; else di = true;
+                    }
+                }
+                umma_commit(&empty_b[bst]);
+                umma_commit(&empty_a[ast]);
+                issued = true;
             }
             if (*abort && issued) {   // the MMAs in flight complete before the columns are freed
                 umma_commit(&fin);
@@ -330,145 +351,152 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             }
         }
     } else {
-        // ---------------- weight builders + epilogue (warps 0-3) ----------------
-        const uint32_t lane_base = tb + ((uint32_t)(32 * warp) << 16);
-        const int m = tid;                  // voxel row of the tile = tensor-memory lane
+        // ---------------- weight builders + epilogue (warps 0-7) ----------------
+        const int grp = warp >> 2;
+        const uint32_t lane_base = tb + ((uint32_t)(32 * (warp & 3)) << 16);
+        const int m = tid & 127;            // voxel row of the tile = tensor-memory lane
         const int lu = m % TC_TU, lv = m / TC_TU;
         const int64_t n_rxkey = g.n_u * g.n_z, n_txkey = g.n_v * g.n_z;
-        uint32_t q = 0, it = 0;
-        for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x, ++it) {
-            const int fb = (int)(item / n_tiles);
-            const int64_t tile = item % n_tiles;
-            const int tz = (int)(tile % J.tiles_z);
-            const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
-            const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
-            const int64_t iz = tz, iu = (int64_t)tu * TC_TU + lu, iv = (int64_t)tv * TC_TV + lv;
-            const bool valid = iz < g.n_z && iu < g.n_u && iv < g.n_v;
-            const int64_t rxkey = valid ? iu * g.n_z + iz : 0;
-            const int64_t txkey = valid ? iv * g.n_z + iz : 0;
-            int cur_tx = -1;
-            float itx = 0.f, ptr = 0.f, pti = 0.f;
-            bool cone = false, any = false;
-            int pre_s = -1;
-            float4 pre_e = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (;;) {
-                const int st = (int)(q % TC_NS);
-                if (!warp_wait(&full_b[st], (q / TC_NS) & 1u, abort)) break;
-                const TcInfo inf = read_info(&info[st]);
-                ++q;
-                if (inf.end) {
-                    mbar_arrive(&full_a[st]);
-                    break;
-                }
-                const int tx = inf.s / g.n_ele, rx = inf.s - tx * g.n_ele;
-                if (tx != cur_tx) {
-                    cur_tx = tx;
-                    const float4 t = valid ? __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey])
-                                           : make_float4(0.f, 0.f, 0.f, 0.f);
-                    itx = t.x; ptr = t.y; pti = t.z;
-                    cone = valid && t.w != 0.0f &&
-                           (g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0);
-                }
-                float4 e;
-                if (pre_s == inf.s) e = pre_e;
-                else e = valid ? __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
-                // the next step's receive entry, loaded while this one is built
-                if (valid && rx + 1 < g.n_ele) {
-                    pre_s = inf.s + 1;
-                    pre_e = __ldg(&g.rx_tab[(int64_t)(rx + 1) * n_rxkey + rxkey]);
-                } else {
-                    pre_s = -1;
-                }
-                const float ab = ab_value(g, tx, rx);
-                const float2 abp = ab_phasor(g, tx, rx);
-                const float idx = __fadd_rn(__fadd_rn(itx, e.x), ab);
-                const float fl = floorf(idx);
-                bool ok = cone && e.w > 0.0f && fl >= (float)KT::LO && fl < (float)(J.n_sample - 1 - KT::HI);
-                int o = ok ? (int)fl - KT::LO - inf.lo : 0;
-                if (ok && (o < 0 || o + TAPS > 16 * inf.nk)) {   // never expected: window bound violated
-                    atomicAdd(prm.err_count, 1ull);
-                    ok = false;
-                    o = 0;
-                }
-                float w[TAPS];
-                poly_weights<KIND, 6>(ok ? idx - fl : 0.0f, w);
-                // P = apod e^{j phi_tx} e^{j phi_rx} e^{j phi_ab} (apod folded in (ar, ai)), scaled
-                const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
-                const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
-                const float py = ok ? TC_SCALE * fmaf(qx, abp.y, qy * abp.x) : 0.0f;
+        int cur_it = -1, fb = 0, cur_tx = -1, pre_s = -1;
+        int64_t iz = 0, iu = 0, iv = 0, rxkey = 0, txkey = 0;
+        bool valid = false, cone = false;
+        float itx = 0.f, ptr = 0.f, pti = 0.f;
+        float4 pre_e = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t q = (uint32_t)grp;; q += TC_GROUPS) {
+            const int bst = (int)(q % TC_NSB);
+            if (!warp_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
+            const TcInfo inf = read_info(&info[bst]);
+            if (inf.kind == TC_FINAL) break;
+            if (inf.it != cur_it) {   // a new item: this thread's voxel
+                cur_it = inf.it;
+                const int64_t item = blockIdx.x + (int64_t)inf.it * gridDim.x;
+                fb = (int)(item / n_tiles);
+                const int64_t tile = item % n_tiles;
+                const int tz = (int)(tile % J.tiles_z);
+                const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
+                const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+                iz = tz; iu = (int64_t)tu * TC_TU + lu; iv = (int64_t)tv * TC_TV + lv;
+                valid = iz < g.n_z && iu < g.n_u && iv < g.n_v;
+                rxkey = valid ? iu * g.n_z + iz : 0;
+                txkey = valid ? iv * g.n_z + iz : 0;
+                cur_tx = -1;
+                pre_s = -1;
+            }
+            const int ast = (int)(q % TC_NSA);
+            // the slot's previous weights have been consumed by their MMAs
+            if (!warp_wait(&empty_a[ast], ((q / TC_NSA) & 1u) ^ 1u, abort)) break;
+            if (inf.kind == TC_END) {
+                mbar_arrive(&full_a[ast]);
+                // ---- epilogue: D_r, D_i -> out (frames of this block) ----
+                if (!warp_wait(&acc_full, (uint32_t)inf.it & 1u, abort)) break;
                 tmem_fence_after_sync();
-                const uint32_t acol = lane_base + (uint32_t)(a_col0 + st * NMAT * 16);
-                auto emit_chunks = [&](const float *v, int nchunk) {
-                    for (int j = 0; j < nchunk; ++j) {
-                        uint32_t rh[8], ih[8];
+                const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
+                for (int c = 0; c < N16; c += 16) {
+                    uint32_t r[16], i16[16];
+                    tmem_ld16(lane_base + (uint32_t)c, r);
+                    tmem_ld16(lane_base + (uint32_t)(N16 + c), i16);
+                    tmem_wait_ld16(r);
+                    tmem_wait_ld16(i16);
+                    if (valid) {
+#pragma unroll
+                        for (int h = 0; h < 8; ++h) {
+                            const int f = fb * FB + c / 2 + h;
+                            if (c / 2 + h < FB && f < J.n_frame) {
+                                float2 val = make_float2(0.f, 0.f);
+                                if (inf.n > 0) {
+                                    val.x = (__uint_as_float(r[2 * h]) - __uint_as_float(i16[2 * h + 1])) *
+                                            (1.0f / TC_SCALE);
+                                    val.y = (__uint_as_float(r[2 * h + 1]) + __uint_as_float(i16[2 * h])) *
+                                            (1.0f / TC_SCALE);
+                                }
+                                float2 *op = J.out + (int64_t)f * g.n_pix + pix;
+                                if (J.accumulate) { float2 x = *op; x.x += val.x; x.y += val.y; *op = x; }
+                                else *op = val;
+                            }
+                        }
+                    }
+                }
+                tmem_fence_before_sync();
+                mbar_arrive(&acc_empty);
+                continue;
+            }
+            const int tx = inf.s / g.n_ele, rx = inf.s - tx * g.n_ele;
+            if (tx != cur_tx) {
+                cur_tx = tx;
+                const float4 t = valid ? __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey])
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+                itx = t.x; ptr = t.y; pti = t.z;
+                cone = valid && t.w != 0.0f && (g.cone_u == nullptr || g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0);
+            }
+            float4 e;
+            if (pre_s == inf.s) e = pre_e;
+            else e = valid ? __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
+            // this group's next record is most often two steps on: its
+            // receive entry is loaded while this one is built
+            if (valid && rx + TC_GROUPS < g.n_ele) {
+                pre_s = inf.s + TC_GROUPS;
+                pre_e = __ldg(&g.rx_tab[(int64_t)(rx + TC_GROUPS) * n_rxkey + rxkey]);
+            } else {
+                pre_s = -1;
+            }
+            const float ab = ab_value(g, tx, rx);
+            const float2 abp = ab_phasor(g, tx, rx);
+            const float idx = __fadd_rn(__fadd_rn(itx, e.x), ab);
+            const float fl = floorf(idx);
+            bool ok = cone && e.w > 0.0f && fl >= (float)KT::LO && fl < (float)(J.n_sample - 1 - KT::HI);
+            int o = ok ? (int)fl - KT::LO - inf.lo : 0;
+            if (ok && (o < 0 || o + TAPS > 16 * inf.nk)) {   // never expected: window bound violated
+                atomicAdd(prm.err_count, 1ull);
+                ok = false;
+                o = 0;
+            }
+            float w[TAPS];
+            poly_weights<KIND, 6>(ok ? idx - fl : 0.0f, w);
+            // P = apod e^{j phi_tx} e^{j phi_rx} e^{j phi_ab} (apod folded in (ar, ai)), scaled
+            const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
+            const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
+            const float py = ok ? TC_SCALE * fmaf(qx, abp.y, qy * abp.x) : 0.0f;
+            tmem_fence_after_sync();
+            const uint32_t acol = lane_base + (uint32_t)(a_col0 + ast * NMAT * 16);
+            auto emit_chunks = [&](const float *v, int nchunk) {
+                for (int j = 0; j < nchunk; ++j) {
+                    uint32_t rh[8], ih[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
+                        rh[c] = tc_pack(a * px, b * px);
+                        ih[c] = tc_pack(a * py, b * py);
+                    }
+                    if constexpr (SPLIT) {
+                        uint32_t rl[8], il[8];
 #pragma unroll
                         for (int c = 0; c < 8; ++c) {
                             const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
-                            rh[c] = tc_pack(a * px, b * px);
-                            ih[c] = tc_pack(a * py, b * py);
+                            rl[c] = tc_pack_rem(a * px, b * px, rh[c]);
+                            il[c] = tc_pack_rem(a * py, b * py, ih[c]);
                         }
-                        if constexpr (SPLIT) {
-                            uint32_t rl[8], il[8];
-#pragma unroll
-                            for (int c = 0; c < 8; ++c) {
-                                const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
-                                rl[c] = tc_pack_rem(a * px, b * px, rh[c]);
-                                il[c] = tc_pack_rem(a * py, b * py, ih[c]);
-                            }
-                            tmem_st8(acol + 0 * 16 + 8 * j, rh);
-                            tmem_st8(acol + 1 * 16 + 8 * j, rl);
-                            tmem_st8(acol + 2 * 16 + 8 * j, ih);
-                            tmem_st8(acol + 3 * 16 + 8 * j, il);
-                        } else {
-                            tmem_st8(acol + 0 * 16 + 8 * j, rh);
-                            tmem_st8(acol + 1 * 16 + 8 * j, ih);
-                        }
-                    }
-                };
-                if (inf.nk == 1) {
-                    float v[16];
-                    tc_place<TAPS, 16>(w, o, v);
-                    emit_chunks(v, 1);
-                } else {
-                    float v[32];
-                    tc_place<TAPS, 32>(w, o, v);
-                    emit_chunks(v, 2);
-                }
-                tmem_wait_st();
-                tmem_fence_before_sync();
-                mbar_arrive(&full_a[st]);
-                any = true;
-            }
-            if (__any_sync(0xffffffffu, *abort != 0)) break;
-            // ---- epilogue: D_r, D_i -> out (frames of this block) ----
-            if (!warp_wait(&acc_full, it & 1u, abort)) break;
-            tmem_fence_after_sync();
-            const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
-            for (int c = 0; c < N16; c += 16) {
-                uint32_t r[16], i16[16];
-                tmem_ld16(lane_base + (uint32_t)c, r);
-                tmem_ld16(lane_base + (uint32_t)(N16 + c), i16);
-                tmem_wait_ld16(r);
-                tmem_wait_ld16(i16);
-                if (valid) {
-#pragma unroll
-                    for (int h = 0; h < 8; ++h) {
-                        const int f = fb * FB + c / 2 + h;
-                        if (c / 2 + h < FB && f < J.n_frame) {
-                            float2 val = make_float2(0.f, 0.f);
-                            if (any) {
-                                val.x = (__uint_as_float(r[2 * h]) - __uint_as_float(i16[2 * h + 1])) * (1.0f / TC_SCALE);
-                                val.y = (__uint_as_float(r[2 * h + 1]) + __uint_as_float(i16[2 * h])) * (1.0f / TC_SCALE);
-                            }
-                            float2 *op = J.out + (int64_t)f * g.n_pix + pix;
-                            if (J.accumulate) { float2 x = *op; x.x += val.x; x.y += val.y; *op = x; }
-                            else *op = val;
-                        }
+                        tmem_st8(acol + 0 * 16 + 8 * j, rh);
+                        tmem_st8(acol + 1 * 16 + 8 * j, rl);
+                        tmem_st8(acol + 2 * 16 + 8 * j, ih);
+                        tmem_st8(acol + 3 * 16 + 8 * j, il);
+                    } else {
+                        tmem_st8(acol + 0 * 16 + 8 * j, rh);
+                        tmem_st8(acol + 1 * 16 + 8 * j, ih);
                     }
                 }
+            };
+            if (inf.nk == 1) {
+                float v[16];
+                tc_place<TAPS, 16>(w, o, v);
+                emit_chunks(v, 1);
+            } else {
+                float v[32];
+                tc_place<TAPS, 32>(w, o, v);
+                emit_chunks(v, 2);
             }
+            tmem_wait_st();
             tmem_fence_before_sync();
-            mbar_arrive(&acc_empty);
+            mbar_arrive(&full_a[ast]);
         }
     }
     if (tid == 0 && *abort) atomicAdd(prm.err_count, 1ull);

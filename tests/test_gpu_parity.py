@@ -389,7 +389,11 @@ def test_autotune_keeps_the_fastest_choice_and_the_result(bf, c2_small):
     plan1 = eng.plan(geom, a3)
     assert plan1["frames_per_block"] == res["frames_per_block"]
     assert plan1["tile"] == [res["tile_u"], res["tile_v"], res["tile_z"]]
-    assert plan1["kernel"] == {0: "fused", 1: "fused_voxel_blocked", 2: "fused_voxel_blocked_tmem"}[res["voxel_blocked"]]
+    if res["tensor_core"]:
+        assert plan1["kernel"] == "fused_tensor_core"
+    else:
+        assert plan1["kernel"] == {0: "fused", 1: "fused_voxel_blocked", 2: "fused_voxel_blocked_tmem"}[
+            res["voxel_blocked"]]
     eng.run(geom, a3)
     torch.cuda.synchronize()
     assert H.rel_rms(after.cpu().numpy(), before.cpu().numpy()) < 1e-4
