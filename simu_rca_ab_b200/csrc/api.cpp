@@ -186,11 +186,21 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
                         : a->kernel == RCABF_KERNEL_FUSED_TC_FP16W ? 1
                                                                    : 0;
     if (want_tc) {
-        const TileShape tts{TC_TILE_U, TC_TILE_V, 1};
         const int fbmax = tc_max_frames_per_block(want_tc == 2);
         bool ok = g->mode == MODE_EXACT && a->storage == RCABF_STORE_F16 && a->compound && !a->per_channel &&
-                  g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_frame >= 32 && a->n_sample >= 2 &&
-                  g->window_rows(tts) <= TC_MAX_ROWS;
+                  g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_frame >= 32 && a->n_sample >= 2;
+        // the 128-voxel tile whose windows are shortest (a forced shape if given)
+        TileShape tts{TC_TILE_U, TC_TILE_V, 1};
+        if (ok) {
+            int best_rows = 1 << 30;
+            const TileShape shapes[] = {{4, 32, 1}, {8, 16, 1}, {2, 64, 1}, {16, 8, 1}, {1, 128, 1}, {32, 4, 1}};
+            for (const TileShape &t : shapes) {
+                if (force && force->ts.tu > 0 && (t.tu != force->ts.tu || t.tv != force->ts.tv)) continue;
+                const int rows = g->window_rows(t);
+                if (rows < best_rows) { best_rows = rows; tts = t; }
+            }
+            ok = best_rows <= TC_MAX_ROWS;
+        }
         int fb = 0;
         if (ok) {
             const int64_t nfb = (a->n_frame + fbmax - 1) / fbmax;
@@ -979,7 +989,6 @@ int rcabf_autotune(const rcabf_geometry *gc, const rcabf_beamform_args *a, void 
         if (!p0.tc) {
             TuneChoice tcc;
             tcc.tc = 2;
-            tcc.ts = TileShape{TC_TILE_U, TC_TILE_V, 1};
             consider(tcc);
         }
         // the one-voxel-per-thread kernel at its own frame blocks

@@ -24,21 +24,26 @@ template <> __device__ __forceinline__ __half2 from_f2<ST_F16>(float2 v) { retur
 template <> __device__ __forceinline__ __nv_bfloat162 from_f2<ST_BF16>(float2 v) { return __float22bfloat162_rn(v); }
 
 constexpr int INGEST_NS = 64;
-constexpr int INGEST_MAX_FB = 64;
+constexpr int INGEST_FCHUNK = 64;    // frames of a block one CTA moves
+constexpr int INGEST_MAX_FB = 128;
 
+// grid.y = frame block x chunk of up to INGEST_FCHUNK of its frames
 template <int STORE, int IQ>
 __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p)
 {
     using T = typename StoreT<STORE>::T;
-    __shared__ float2 tile[INGEST_MAX_FB][INGEST_NS + 1];
+    __shared__ float2 tile[INGEST_FCHUNK][INGEST_NS + 1];
     const int n_base = blockIdx.x * INGEST_NS;
-    const int fb = blockIdx.y;
+    const int n_chunk = (p.fb + INGEST_FCHUNK - 1) / INGEST_FCHUNK;
+    const int fb = blockIdx.y / n_chunk;
+    const int f0 = (blockIdx.y % n_chunk) * INGEST_FCHUNK;   // first frame of the chunk within the block
     const int te = blockIdx.z;
     const int tx = te / p.n_ele, ele = te % p.n_ele;
     const int FB = p.fb;
-    for (int i = threadIdx.x; i < FB * INGEST_NS; i += blockDim.x) {
+    const int FC = min(INGEST_FCHUNK, FB - f0);              // frames of this chunk
+    for (int i = threadIdx.x; i < FC * INGEST_NS; i += blockDim.x) {
         const int fi = i / INGEST_NS, nl = i % INGEST_NS;
-        const int64_t f = (int64_t)fb * FB + fi;
+        const int64_t f = (int64_t)fb * FB + f0 + fi;
         const int n = n_base + nl;
         float2 v = make_float2(0.f, 0.f);
         if (f < p.n_frame && n < p.n_sample)
@@ -49,17 +54,18 @@ __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p)
     T *slab = reinterpret_cast<T *>(reinterpret_cast<char *>(p.S) +
                                     (((int64_t)tx * p.n_ele + ele) * p.n_fb + fb) * p.slab_bytes);
     const int n_rows = max(p.n_rows, p.n_sample);
-    for (int i = threadIdx.x; i < FB * INGEST_NS; i += blockDim.x) {
-        const int nl = i / FB, fi = i % FB;
+    for (int i = threadIdx.x; i < FC * INGEST_NS; i += blockDim.x) {
+        const int nl = i / FC, fi = i % FC;
         const int n = n_base + nl;
-        if (n < n_rows) slab[(int64_t)n * FB + fi] = from_f2<STORE>(tile[fi][nl]);   // zeros past the record
+        if (n < n_rows) slab[(int64_t)n * FB + f0 + fi] = from_f2<STORE>(tile[fi][nl]);   // zeros past the record
     }
 }
 
 template <int STORE>
 static cudaError_t launch_ingest_store(const IngestParams &p, cudaStream_t st)
 {
-    dim3 grid((std::max(p.n_rows, p.n_sample) + INGEST_NS - 1) / INGEST_NS, p.n_fb, p.n_tx * p.n_ele);
+    const int n_chunk = (p.fb + INGEST_FCHUNK - 1) / INGEST_FCHUNK;
+    dim3 grid((std::max(p.n_rows, p.n_sample) + INGEST_NS - 1) / INGEST_NS, p.n_fb * n_chunk, p.n_tx * p.n_ele);
     switch (p.iq_dtype) {
     case 0: ingest_kernel<STORE, 0><<<grid, 256, 0, st>>>(p); break;
     case 1: ingest_kernel<STORE, 1><<<grid, 256, 0, st>>>(p); break;
@@ -72,7 +78,8 @@ static cudaError_t launch_ingest_store(const IngestParams &p, cudaStream_t st)
 
 cudaError_t launch_ingest(const IngestParams &p, int store, cudaStream_t st)
 {
-    if (p.fb < 1 || p.fb > INGEST_MAX_FB || p.n_fb > 65535 || p.n_tx * p.n_ele > 65535)
+    if (p.fb < 1 || p.fb > INGEST_MAX_FB || (int64_t)p.n_fb * ((p.fb + INGEST_FCHUNK - 1) / INGEST_FCHUNK) > 65535 ||
+        p.n_tx * p.n_ele > 65535)
         return cudaErrorInvalidValue;
     switch (store) {
     case ST_F32: return launch_ingest_store<ST_F32>(p, st);

@@ -1,8 +1,9 @@
 // Delay-and-sum on the tensor cores (sm_100a tcgen05.mma), EXACT tables,
 // FP16 slabs, rectilinear grids, transmits compounded.
 //
-// Formulation.  For a tile of 128 voxels (TU along the receive axis x TV
-// along the steering axis, one depth) and one (tx, rx) step, the sample
+// Formulation.  For a tile of 128 voxels (tu along the receive axis x tv
+// along the steering axis, one depth; the planner picks the shape whose
+// windows are shortest) and one (tx, rx) step, the sample
 // rows every voxel of the tile touches form one window [lo, lo + K) of the
 // step's slab, K <= 32 rows.  With W[m][k] = P_m w_m(k - o_m) (the voxel's
 // interpolation weights placed at its own row offset o_m inside the window,
@@ -56,9 +57,7 @@ namespace rcabf {
 constexpr int TC_GROUPS = 2;               // builder groups of 4 warps
 constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
 constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
-constexpr int TC_TU = TC_TILE_U, TC_TV = TC_TILE_V;   // tile: TU (receive axis) x TV (steering axis) x 1 depth
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
-static_assert(TC_TU * TC_TV == 128, "one voxel per tensor-memory lane");
 constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
 constexpr int TC_NSB = 12;                 // window stages in shared memory
 constexpr int TC_PANEL_BYTES = TC_KCH * 2048;   // one 64-element panel of B: TC_KCH x (16 rows x 128 B)
@@ -193,7 +192,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         unsigned dyn;
         asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
         if (dyn < (unsigned)tc_smem_bytes(FB) || tc_tmem_cols(FB, SPLIT) > 512 || NH < 64 || (FB & 7) ||
-            J.compound == 0) {
+            J.compound == 0 || J.tu * J.tv != 128 || J.tz != 1) {
             if (tid == 0) atomicAdd(prm.err_count, 1ull);
             return;
         }
@@ -355,7 +354,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         const int grp = warp >> 2;
         const uint32_t lane_base = tb + ((uint32_t)(32 * (warp & 3)) << 16);
         const int m = tid & 127;            // voxel row of the tile = tensor-memory lane
-        const int lu = m % TC_TU, lv = m / TC_TU;
+        const int lu = m % J.tu, lv = m / J.tu;
         const int64_t n_rxkey = g.n_u * g.n_z, n_txkey = g.n_v * g.n_z;
         int cur_it = -1, fb = 0, cur_tx = -1, pre_s = -1;
         int64_t iz = 0, iu = 0, iv = 0, rxkey = 0, txkey = 0;
@@ -375,7 +374,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 const int tz = (int)(tile % J.tiles_z);
                 const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
                 const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
-                iz = tz; iu = (int64_t)tu * TC_TU + lu; iv = (int64_t)tv * TC_TV + lv;
+                iz = tz; iu = (int64_t)tu * J.tu + lu; iv = (int64_t)tv * J.tv + lv;
                 valid = iz < g.n_z && iu < g.n_u && iv < g.n_v;
                 rxkey = valid ? iu * g.n_z + iz : 0;
                 txkey = valid ? iv * g.n_z + iz : 0;

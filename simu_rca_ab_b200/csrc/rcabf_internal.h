@@ -88,9 +88,10 @@ struct FusedJob {
     int32_t tu, tv, tz;        // tile shape, tu*tv*tz = blockDim.x
 };
 
-// Tensor-core kernel (fused_tc_kernel.cuh): voxel tile TC_TILE_U (receive
-// axis) x TC_TILE_V (steering axis) x 1 depth, windows of at most
-// TC_MAX_ROWS sample rows per (tx, rx) step.
+// Tensor-core kernel (fused_tc_kernel.cuh): voxel tiles of 128 voxels, tu
+// (receive axis) x tv (steering axis) x 1 depth, with windows of at most
+// TC_MAX_ROWS sample rows per (tx, rx) step; TC_TILE_U x TC_TILE_V is the
+// preferred shape.
 constexpr int TC_TILE_U = 4, TC_TILE_V = 32, TC_MAX_ROWS = 32;
 
 constexpr int MAX_JOBS = 24;
