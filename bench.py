@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-serving-plain", action="store_true", help="skip serving the stream on the plain kernel")
     ap.add_argument("--plain-frames", type=int, default=10)
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference kernel on the GPU")
+    ap.add_argument("--no-tc16", action="store_true",
+                    help="skip the tensor-core kernel with single FP16 weights (timed beside the default)")
     ap.add_argument("--ref-gpu-frames", type=int, default=20,
                     help="frames of the workload the reference GPU kernel is timed on")
     ap.add_argument("--cpu-sample-frames", type=int, default=4)
@@ -373,6 +375,23 @@ def simulator_leg(dev, seed: int = 7):
                     f"{n_scat} scatterers, {n_frame} frames, {p['n_freq']} frequencies, Raw {list(raw.shape)}",
             "ms": 1e3 * el, "element_field_terms_per_s": evals / el,
             "note": "scatterers static within a frame: one element field per frame, all transmits as one GEMM"}
+
+
+def tensor_peak():
+    """Dense FP16/BF16 tensor peak (TFLOP/s) and where it comes from: the
+    pool's measured figure (sustained: the kernel runs inside a long step)
+    when MEASURED_PEAKS.json is present, else the pool's earlier burst
+    measurement."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            d = json.loads(f.read_text())
+            for k in ("bf16_tflops_sustained", "bf16_tflops"):
+                if d.get(k):
+                    return float(d[k]), f"MEASURED_PEAKS.json {k} (of measured)"
+        except (ValueError, OSError):
+            pass
+    return 1590.0, "1.59 PFLOP/s dense bf16 burst, an earlier measurement on this pool (of fallback)"
 
 
 def ref_gpu_leg(w, data, frames: int, variant: str = "fast"):
@@ -686,6 +705,39 @@ def main():
                  "ratio": (value / world) / p_val}
         del p_in, p_out
 
+    # the tensor-core kernel with single FP16 weights (chosen by name only):
+    # the same step, timed, and its error against the FP64 oracle below
+    tc16, out16 = None, None
+    if not a.no_tc16 and plan.get("kernel") == "fused_tensor_core" and rank == 0:
+        try:
+            out16 = torch.empty_like(out)
+            a16 = [eng.make_args(g, iq_dev[gi], iq_dtype=iq_code, n_sample=w.n_sample, n_frame=F, out=out16,
+                                 mask=None, compound=True, storage=st_code, kernel=L.KERNEL_FUSED_TC_FP16W,
+                                 accumulate=gi > 0) for gi, g in enumerate(geoms)]
+            ws16 = [torch.empty(max(256, eng.workspace_bytes(g, ar)), dtype=torch.uint8, device=dev)
+                    for g, ar in zip(geoms, a16)]
+
+            def step16():
+                for g, ar, wsp in zip(geoms, a16, ws16):
+                    eng.run(g, ar, stream=stream, workspace=wsp)
+
+            step16()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(a.steps):
+                step16()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms16 = e0.elapsed_time(e1) / a.steps
+            tc16 = {"kernel": "fused_tc_kernel, single FP16 weights (RCABF_KERNEL_FUSED_TC_FP16W)",
+                    "ms_per_step": ms16, "value": units / (ms16 * 1e-3), "unit": UNIT,
+                    "plan": eng.plan(geoms[0], a16[0])}
+            del ws16
+        except Exception as ex:
+            tc16 = {"error": f"{type(ex).__name__}: {ex}"}
+            out16 = None
+
     ref_gpu = None
     if not a.no_ref_gpu and rank == 0:
         try:
@@ -733,16 +785,31 @@ def main():
         active *= F
         fpu = 8 * w.lanczos_a + 8
         achieved = active * fpu / (fused_ms * 1e-3) / 1e12
+        kname = KERNEL_NAMES.get(plan.get("kernel"), plan.get("kernel"))
         traffic = None
-        tf = ROOT / "profiles" / f"traffic_{w.name}_{storage}.json"
+        tf = ROOT / "profiles" / f"traffic_{kname}_{w.name}_{storage}.json"
         if tf.exists():
             traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
-        roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                "frac": achieved / peak.value, "traffic": traffic,
+        fp32 = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                "frac": achieved / peak.value,
                 "peak_source": "FP32 FMA probe kernel timed live in this run (MEASURED_PEAKS.json has no FP32 figure)",
-                "kernel": KERNEL_NAMES.get(plan.get("kernel"), plan.get("kernel")), "kernel_ms": fused_ms,
                 "work": f"{active:.4e} active units x {fpu} FLOP ({active / (units):.3f} of nominal)",
                 "nominal_achieved": units * fpu / (fused_ms * 1e-3) / 1e12}
+        mma = sum(eng.plan(g, ar).get("mma_flops", 0.0) for g, ar in zip(geoms, args))
+        if mma > 0:
+            # the tensor-core kernel: its dense MMA work (the banded products
+            # as issued, counted exactly from the windows) against the tensor
+            # peak; the algorithmic FP32 work it stands for is fp32_equivalent
+            tpk, tsrc = tensor_peak()
+            ach_t = mma / (fused_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "achieved": ach_t, "peak": tpk, "unit": "TFLOP/s", "frac": ach_t / tpk,
+                    "traffic": traffic, "peak_source": tsrc, "kernel": kname, "kernel_ms": fused_ms,
+                    "work": f"{mma:.4e} dense MMA FLOPs per step (16-row window chunks x weight matrices x "
+                            f"2 x 128 x N x 16, N = 2 x frames per block)",
+                    "fp32_equivalent": fp32}
+        else:
+            roof = dict(fp32)
+            roof.update({"traffic": traffic, "kernel": kname, "kernel_ms": fused_ms})
         acc = None
         if not a.no_accuracy:
             rng = np.random.default_rng(123)
@@ -760,6 +827,9 @@ def main():
             rms, pk = H.error_db(ours, ref)
             acc = {"rms_db": rms, "peak_db": pk, "vs": "FP64 oracle (complex64 input before storage rounding)",
                    "sample": f"{pix.size} random voxels x frames {frames}"}
+            if tc16 is not None and out16 is not None:
+                r16, p16 = H.error_db(out16[frames][:, 0, :].cpu().numpy()[:, pix], ref)
+                tc16.update({"rms_db": r16, "peak_db": p16})
         cb = None
         if not a.no_cpu_baseline:
             dnp = data[: a.cpu_sample_frames].cpu().numpy()
@@ -778,6 +848,7 @@ def main():
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain, "reference_gpu": ref_gpu,
             "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim, "ulm": ulm,
+            "tensor_core_fp16_weights": tc16,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }
         print(json.dumps(line), flush=True)

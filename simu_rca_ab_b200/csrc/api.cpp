@@ -181,14 +181,21 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     // rows, at least 32 frames; frame blocks of a multiple of 8 frames, as
     // few as the tensor-memory budget allows (the weights are built once
     // per block).
-    const int want_tc = force ? force->tc
-                        : a->kernel == RCABF_KERNEL_FUSED_TC       ? 2
-                        : a->kernel == RCABF_KERNEL_FUSED_TC_FP16W ? 1
-                                                                   : 0;
+    // The planner's own choice (kernel AUTO / FUSED, no frame block asked
+    // for) takes it, with hi + remainder weights, where it applies to 32
+    // frames or more; by name or by a stored / forced choice it also takes
+    // fewer frames (one padded block).
+    const int named_tc = force ? force->tc
+                         : a->kernel == RCABF_KERNEL_FUSED_TC       ? 2
+                         : a->kernel == RCABF_KERNEL_FUSED_TC_FP16W ? 1
+                                                                    : 0;
+    const bool auto_tc = !named_tc && !force && fb_req == 0 &&
+                         (a->kernel == RCABF_KERNEL_AUTO || a->kernel == RCABF_KERNEL_FUSED) && a->n_frame >= 32;
+    const int want_tc = named_tc ? named_tc : auto_tc ? 2 : 0;
     if (want_tc) {
         const int fbmax = tc_max_frames_per_block(want_tc == 2);
         bool ok = g->mode == MODE_EXACT && a->storage == RCABF_STORE_F16 && a->compound && !a->per_channel &&
-                  g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_frame >= 32 && a->n_sample >= 2;
+                  g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_sample >= 2;
         // the 128-voxel tile whose windows are shortest (a forced shape if given)
         TileShape tts{TC_TILE_U, TC_TILE_V, 1};
         if (ok) {
@@ -223,7 +230,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
             return RCABF_OK;
         }
         p = Plan{};
-        return RCABF_ERR_UNSUPPORTED;
+        if (named_tc) return RCABF_ERR_UNSUPPORTED;
+        p.kernel = RCABF_KERNEL_FUSED;   // not tensor-core work: the SIMT kernels below
+        p.store = a->storage;
     }
 
     // Voxel-blocked kernel: exact tables, a steering axis to block along,
@@ -661,12 +670,21 @@ int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, c
                         : p.vb == 2                     ? "fused_voxel_blocked_tmem"
                         : p.vb                          ? "fused_voxel_blocked"
                                                         : "fused";
+    // tensor-core plans: the MMA work of one call, counted on the host
+    double mma_flops = 0.0;
+    if (p.tc) {
+        const int64_t chunks = const_cast<rcabf_geometry *>(g)->tc_chunks(p.ts, a->n_sample);
+        const int nmat = p.tc == 2 ? 4 : 2;
+        const int n16 = (2 * p.fb + 15) / 16 * 16;
+        mma_flops = (double)chunks * p.n_fb * nmat * 2.0 * 128.0 * n16 * 16.0;
+    }
     snprintf(buf, len,
              "{\"kernel\": \"%s\", \"row_shift\": %d, \"frames_per_block\": %d, \"frame_blocks\": %d, "
              "\"tile\": [%d, %d, %d], \"voxels_per_thread\": %d, \"window_rows\": %d, \"smem_bytes\": %zu, "
-             "\"workspace_bytes\": %zu, \"work_items\": %lld, \"storage\": %d, \"ctas_per_sm\": %d}",
+             "\"workspace_bytes\": %zu, \"work_items\": %lld, \"storage\": %d, \"ctas_per_sm\": %d, "
+             "\"mma_flops\": %.6e}",
              kname, p.d, p.fb, p.n_fb, p.ts.tu, p.vb ? p.ts.tv * VB_BLOCK : p.ts.tv, p.ts.tz, p.vb ? VB_BLOCK : 1,
-             p.wmax, p.smem, p.total, (long long)p.n_items, p.store, occ);
+             p.wmax, p.smem, p.total, (long long)p.n_items, p.store, occ, mma_flops);
     return RCABF_OK;
 }
 
@@ -723,6 +741,12 @@ int host_layout(rcabf_geometry *g, const rcabf_beamform_args *a, int32_t frames_
             h.have_tuned = true;
             h.tuned = it->second;
         }
+    }
+    if (p.tc && !h.have_tuned) {   // every chunk on the tensor-core kernel (its frame block its own)
+        h.have_tuned = true;
+        h.tuned = TuneChoice{};
+        h.tuned.tc = p.tc;
+        h.tuned.ts = p.ts;
     }
     const int64_t n_t = a->compound ? 1 : a->n_tx;
     h.in_bytes = align256((size_t)h.chunk * a->n_tx * a->n_ch * a->n_sample * iq_sample_bytes(a->iq_dtype));

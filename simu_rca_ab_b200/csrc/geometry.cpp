@@ -489,6 +489,62 @@ int rcabf_geometry::window_rows(const rcabf::TileShape &ts)
     return (int)std::ceil(m) + rcabf::kind_taps(kind) + 3;
 }
 
+int64_t rcabf_geometry::tc_chunks(const rcabf::TileShape &ts, int64_t n_sample)
+{
+    std::lock_guard<std::mutex> lk(mu);
+    const std::array<int64_t, 3> key{ts.tu, ts.tv, n_sample};
+    auto it = tc_chunk_counts.find(key);
+    if (it != tc_chunk_counts.end()) return it->second;
+    const int64_t tiles_u = (n_u + ts.tu - 1) / ts.tu, tiles_v = (n_v + ts.tv - 1) / ts.tv;
+    const int lo_taps = rcabf::kind_lo(kind), taps = rcabf::kind_taps(kind);
+    // per (element, u tile, z) and (transmit, v tile, z): min / max table delay
+    // of the valid entries (as the window-range kernel forms them)
+    auto ranges = [&](const std::vector<float> &tab, int64_t rows, int64_t n_a, int64_t ta, int64_t tiles_a,
+                      std::vector<float> &mn, std::vector<float> &mx) {
+        mn.assign((size_t)(rows * tiles_a * n_z), INFINITY);
+        mx.assign((size_t)(rows * tiles_a * n_z), -INFINITY);
+        for (int64_t r = 0; r < rows; ++r)
+            for (int64_t a = 0; a < n_a; ++a)
+                for (int64_t z = 0; z < n_z; ++z) {
+                    const float v = tab[(size_t)(r * n_a * n_z + a * n_z + z)];
+                    if (std::isnan(v)) continue;
+                    const size_t o = (size_t)((r * tiles_a + a / ta) * n_z + z);
+                    mn[o] = std::min(mn[o], v);
+                    mx[o] = std::max(mx[o], v);
+                }
+    };
+    std::vector<float> rmn, rmx, tmn, tmx;
+    ranges(rx_delay, n_ele, n_u, ts.tu, tiles_u, rmn, rmx);
+    ranges(tx_delay, n_tx, n_v, ts.tv, tiles_v, tmn, tmx);
+    int64_t total = 0;
+    const float fmax_n = (float)n_sample;
+    for (int64_t t = 0; t < n_tx; ++t)
+        for (int64_t e = 0; e < n_ele; ++e) {
+            const float ab = ab_host.empty() ? 0.0f : ab_host[(size_t)(ab_per_tx ? t * n_ele + e : e)];
+            for (int64_t tu = 0; tu < tiles_u; ++tu)
+                for (int64_t z = 0; z < n_z; ++z) {
+                    const size_t ro = (size_t)((e * tiles_u + tu) * n_z + z);
+                    if (!(rmn[ro] <= rmx[ro])) continue;
+                    for (int64_t tv = 0; tv < tiles_v; ++tv) {
+                        const size_t to = (size_t)((t * tiles_v + tv) * n_z + z);
+                        if (!(tmn[to] <= tmx[to])) continue;
+                        volatile float l0 = tmn[to] + rmn[ro];
+                        volatile float h0 = tmx[to] + rmx[ro];
+                        float lo_f = l0 + ab, hi_f = h0 + ab;
+                        lo_f = std::min(std::max(std::floor(lo_f), -1.0f), fmax_n);
+                        hi_f = std::min(std::max(std::floor(hi_f), -1.0f), fmax_n);
+                        const int l = std::max((int)lo_f - lo_taps, 0);
+                        const int h = std::min((int)hi_f - lo_taps + taps - 1, (int)n_sample - 2);
+                        if (h < l) continue;
+                        const int nk = (h - l + 1 + 15) / 16;
+                        if (nk <= rcabf::TC_MAX_ROWS / 16) total += nk;
+                    }
+                }
+        }
+    tc_chunk_counts[key] = total;
+    return total;
+}
+
 int rcabf_geometry::vb_shift(int block)
 {
     std::lock_guard<std::mutex> lk(mu);

@@ -78,6 +78,13 @@ struct rcabf_geometry {
     // (tx, ele) step: spread of the transmit delay + spread of the receive
     // delay inside the tile (in samples) + the taps + rounding slack.
     int window_rows(const rcabf::TileShape &ts);
+    // Tensor-core kernel: the 16-row window chunks its producer issues for
+    // one frame block over all tiles of this shape and all (tx, element)
+    // steps -- the same window arithmetic as the kernel, on the host copies
+    // of the table delays -- i.e. its MMA work (each chunk is NMAT MMAs of
+    // 128 x 2 FB x 16).
+    int64_t tc_chunks(const rcabf::TileShape &ts, int64_t n_sample);
+    std::map<std::array<int64_t, 3>, int64_t> tc_chunk_counts;
     // Largest difference of floor(sample index) between voxels of one
     // aligned block of `block` consecutive v (same u, z, tx, rx), i.e. the
     // row shift bound D of the voxel-blocked kernel; -1 if not applicable.
