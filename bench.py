@@ -252,12 +252,22 @@ def serving_leg(eng, dev, n_requests: int, rates, seed: int = 3, plain: bool = T
     torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(min(150e9, free - 8e9))
+    # the arena is one allocation: step down until the device grants it
+    while True:
+        try:
+            Server(eng, budget, n_streams=1, max_queue=1, max_batch=1).close()
+            break
+        except L.RcabfError:
+            if budget < 16e9:
+                raise
+            budget = int(budget * 0.9)
     res = {"workload": f"c3 serving mix: {n_requests} requests per stream, Poisson arrivals (seed {seed}); probe "
                        "64+64 or 128+128, 1-32 tx, 1-64 frames, grids 32x32x64..128x128x256, FP32/FP16 storage, "
                        "f-number 1.5, Lanczos a=3; channel data and geometry tables resident",
            "hbm_budget_bytes": budget,
            "hbm_budget_note": "150 GB as configured" if budget >= 150e9 else
-                              f"150 GB configured; {free / 1e9:.1f} GB free on the device, 8 GB kept back",
+                              f"150 GB configured; {free / 1e9:.1f} GB free on the device; the largest arena the "
+                              f"device granted in one allocation, 8 GB kept back",
            "rates": []}
     items0 = None
     for rate in sorted(rates):

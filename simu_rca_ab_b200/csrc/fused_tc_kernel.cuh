@@ -23,15 +23,16 @@
 // FP16 rounding (~11 bits).  All weights are scaled by 2^8 (undone in the
 // epilogue) so that the remainder terms stay out of the FP16 subnormal range.
 //
-// Roles (320 threads): two groups of four warps build the weight matrices,
-// one voxel per thread, straight into tensor memory (lane = voxel row;
-// tcgen05.st), alternating records (group 0 the even ones, group 1 the odd
-// ones, so that one group's setup overlaps the other's), and the group that
-// meets an item's end record writes that item's outputs; warp 8 computes
+// Roles (448 threads): three groups of four warps build the weight
+// matrices, one voxel per thread, straight into tensor memory (lane = voxel
+// row; tcgen05.st), taking records in turn (group g the records q with
+// q mod 3 = g, so that the groups' dependent setup chains overlap), and the
+// group that
+// meets an item's end record writes that item's outputs; warp 12 computes
 // the windows of 32 steps at a time and loads each active step's window with
 // 2-D TMA (128-byte swizzle) into a ring of TC_NSB shared-memory stages, up
 // to TC_NSB records ahead of the MMAs, so the load latency stays off the
-// critical path; warp 9 issues the MMAs (A from one of TC_NSA tensor-memory
+// critical path; warp 13 issues the MMAs (A from one of TC_NSA tensor-memory
 // weight slots, B from shared memory) and commits them to the slot's and
 // the stage's "empty" barriers.  Steps whose window is empty for the whole
 // tile are skipped by every role alike: the producer passes each active
@@ -54,7 +55,7 @@
 
 namespace rcabf {
 
-constexpr int TC_GROUPS = 2;               // builder groups of 4 warps
+constexpr int TC_GROUPS = 3;               // builder groups of 4 warps
 constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
 constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
@@ -85,14 +86,14 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volati
 // TC_FINAL (no more items).  it counts the CTA's items.
 enum TcKind : int32_t { TC_STEP = 0, TC_END = 1, TC_FINAL = 2 };
 struct TcInfo {
-    int32_t kind, s, lo, nk, it, n;
+    int32_t kind, s, lo, nk, it, n, tx, rx;
 };
 // a record written by another thread (published through an mbarrier)
 __device__ __forceinline__ TcInfo read_info(const TcInfo *p)
 {
     const volatile TcInfo *v = p;
     TcInfo r;
-    r.kind = v->kind; r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.it = v->it; r.n = v->n;
+    r.kind = v->kind; r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.it = v->it; r.n = v->n; r.tx = v->tx; r.rx = v->rx;
     return r;
 }
 
@@ -283,13 +284,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     const int lo_i = __shfl_sync(0xffffffffu, lo, i);
                     const int nk_i = __shfl_sync(0xffffffffu, nk, i);
                     const int64_t row0 = ((int64_t)(s0 + i) * J.n_fb + fb) * prm.rows_per_slab + lo_i;
-                    emit(TcInfo{TC_STEP, s0 + i, lo_i, nk_i, it, 0}, row0);
+                    const int tx_i = (s0 + i) / g.n_ele;
+                    emit(TcInfo{TC_STEP, s0 + i, lo_i, nk_i, it, 0, tx_i, s0 + i - tx_i * g.n_ele}, row0);
                     ++n_active;
                 }
             }
-            if (!stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active}, 0);
+            if (!stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
         }
-        for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0}, 0);
+        for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
         if (lane == 0 && stop) {
             // let the copies in flight land before the CTA's shared memory goes
             for (int st = 0; st < TC_NSB; ++st)
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             }
         }
     } else {
-        // ---------------- weight builders + epilogue (warps 0-7) ----------------
+        // ---------------- weight builders + epilogue (warps 0 .. 4 TC_GROUPS - 1) ----------------
         const int grp = warp >> 2;
         const uint32_t lane_base = tb + ((uint32_t)(32 * (warp & 3)) << 16);
         const int m = tid & 127;            // voxel row of the tile = tensor-memory lane
@@ -419,7 +421,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 mbar_arrive(&acc_empty);
                 continue;
             }
-            const int tx = inf.s / g.n_ele, rx = inf.s - tx * g.n_ele;
+            const int tx = inf.tx, rx = inf.rx;
             if (tx != cur_tx) {
                 cur_tx = tx;
                 const float4 t = valid ? __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey])
