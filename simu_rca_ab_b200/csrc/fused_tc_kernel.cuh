@@ -49,6 +49,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "das_common.cuh"
 #include "poly_weights.cuh"
 #include "tc_common.cuh"
@@ -384,9 +386,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 pre_s = -1;
             }
             const int ast = (int)(q % TC_NSA);
-            // the slot's previous weights have been consumed by their MMAs
-            if (!warp_wait(&empty_a[ast], ((q / TC_NSA) & 1u) ^ 1u, abort)) break;
+            const uint32_t a_par = ((q / TC_NSA) & 1u) ^ 1u;   // the slot's previous use has been consumed
             if (inf.kind == TC_END) {
+                if (!warp_wait(&empty_a[ast], a_par, abort)) break;
                 mbar_arrive(&full_a[ast]);
                 // ---- epilogue: D_r, D_i -> out (frames of this block) ----
                 if (!warp_wait(&acc_full, (uint32_t)inf.it & 1u, abort)) break;
@@ -457,46 +459,47 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
             const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
             const float py = ok ? TC_SCALE * fmaf(qx, abp.y, qy * abp.x) : 0.0f;
-            tmem_fence_after_sync();
             const uint32_t acol = lane_base + (uint32_t)(a_col0 + ast * NMAT * 16);
-            auto emit_chunks = [&](const float *v, int nchunk) {
-                for (int j = 0; j < nchunk; ++j) {
-                    uint32_t rh[8], ih[8];
+            // the packed weight rows are formed in registers first; the wait
+            // for the slot comes only before the stores, so that a group's
+            // arithmetic overlaps the MMAs still reading the slot
+            auto build = [&](auto nkc) -> bool {
+                constexpr int NKC = decltype(nkc)::value;
+                float v[16 * NKC];
+                tc_place<TAPS, 16 * NKC>(w, o, v);
+                uint32_t words[NMAT][8 * NKC];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) {
-                        const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
-                        rh[c] = tc_pack(a * px, b * px);
-                        ih[c] = tc_pack(a * py, b * py);
-                    }
+                for (int c = 0; c < 8 * NKC; ++c) {
+                    const float ar = v[2 * c] * px, br = v[2 * c + 1] * px;
+                    const float ai = v[2 * c] * py, bi = v[2 * c + 1] * py;
                     if constexpr (SPLIT) {
-                        uint32_t rl[8], il[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {
-                            const float a = v[16 * j + 2 * c], b = v[16 * j + 2 * c + 1];
-                            rl[c] = tc_pack_rem(a * px, b * px, rh[c]);
-                            il[c] = tc_pack_rem(a * py, b * py, ih[c]);
-                        }
-                        tmem_st8(acol + 0 * 16 + 8 * j, rh);
-                        tmem_st8(acol + 1 * 16 + 8 * j, rl);
-                        tmem_st8(acol + 2 * 16 + 8 * j, ih);
-                        tmem_st8(acol + 3 * 16 + 8 * j, il);
+                        words[0][c] = tc_pack(ar, br);
+                        words[1][c] = tc_pack_rem(ar, br, words[0][c]);
+                        words[2][c] = tc_pack(ai, bi);
+                        words[3][c] = tc_pack_rem(ai, bi, words[2][c]);
                     } else {
-                        tmem_st8(acol + 0 * 16 + 8 * j, rh);
-                        tmem_st8(acol + 1 * 16 + 8 * j, ih);
+                        words[0][c] = tc_pack(ar, br);
+                        words[1][c] = tc_pack(ai, bi);
                     }
                 }
+                if (!warp_wait(&empty_a[ast], a_par, abort)) return false;
+                tmem_fence_after_sync();
+#pragma unroll
+                for (int mat = 0; mat < NMAT; ++mat)
+#pragma unroll
+                    for (int j = 0; j < NKC; ++j) {
+                        uint32_t r8[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) r8[c] = words[mat][8 * j + c];
+                        tmem_st8(acol + (uint32_t)(mat * 16 + 8 * j), r8);
+                    }
+                tmem_wait_st();
+                tmem_fence_before_sync();
+                return true;
             };
-            if (inf.nk == 1) {
-                float v[16];
-                tc_place<TAPS, 16>(w, o, v);
-                emit_chunks(v, 1);
-            } else {
-                float v[32];
-                tc_place<TAPS, 32>(w, o, v);
-                emit_chunks(v, 2);
-            }
-            tmem_wait_st();
-            tmem_fence_before_sync();
+            const bool built = inf.nk == 1 ? build(std::integral_constant<int, 1>{})
+                                           : build(std::integral_constant<int, 2>{});
+            if (!built) break;
             mbar_arrive(&full_a[ast]);
         }
     }

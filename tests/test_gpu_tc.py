@@ -154,8 +154,8 @@ def test_accumulate_adds_into_the_output(c2_40):
 
 
 def test_declined_cases(c2_40):
-    """Per-transmit output, FP32 storage and fewer than 32 frames are not
-    tensor-core work: the call is refused (RCABF_ERR_UNSUPPORTED)."""
+    """Per-transmit output and FP32 storage are not tensor-core work: the call
+    is refused (RCABF_ERR_UNSUPPORTED)."""
     from simu_rca_ab_b200 import _lib as L
     from simu_rca_ab_b200 import workloads as W
     w, data, eng, geom, iq = c2_40
@@ -163,6 +163,12 @@ def test_declined_cases(c2_40):
         _run(w, eng, geom, iq, L.KERNEL_FUSED_TC, compound=False)
     with pytest.raises(Exception):
         _run(w, eng, geom, data.contiguous(), L.KERNEL_FUSED_TC, storage=L.STORE_F32)
+    # by name it also takes fewer than 32 frames (one block padded to 32);
+    # the planner's own choice leaves those to the SIMT kernels
     w8 = W.get("c2", n_frame=8)
-    with pytest.raises(Exception):
-        _run(w8, eng, geom, iq[:8].contiguous(), L.KERNEL_FUSED_TC)
+    out8, plan8 = _run(w8, eng, geom, iq[:8].contiguous(), L.KERNEL_FUSED_TC)
+    assert plan8["kernel"] == "fused_tensor_core" and plan8["frames_per_block"] == 32
+    ref8, plan_auto = _run(w8, eng, geom, iq[:8].contiguous(), L.KERNEL_AUTO)
+    assert not plan_auto["kernel"].startswith("fused_tensor_core")
+    assert H.rel_rms(out8.cpu().numpy(), ref8.cpu().numpy()) < 2e-4
+    assert _errcount() == 0
