@@ -80,14 +80,20 @@ cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, in
     p.rows_per_slab = rows_per_slab;
     p.n_items = n_items;
     p.err_count = err;
-    // the slabs as one 2-D FP16 tensor: rows of 2 fb halfs, one box = 64
-    // halfs x 16 rows, 128-byte swizzle (the MMA's B layout); columns past
-    // 2 fb (the last panel) read as zeros
-    cuuint64_t dims[2] = {(cuuint64_t)(2 * fb), (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(4 * fb)};
-    cuuint32_t box[2] = {64, 16};
-    cuuint32_t es[2] = {1, 1};
-    const CUresult cr = enc(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(job.S), dims, strides, box,
+    // the slabs as a 3-D FP16 tensor: x = element within a 64-element
+    // panel of a row (2-byte stride), y = row (rows of 2 fb halfs), z = panel
+    // (128-byte stride); one box = one 16-row chunk of every panel, laid out
+    // panel after panel with the 128-byte swizzle (the MMA's B layout).  The
+    // last panel reaches past the row end into the next row: those columns
+    // (>= 2 fb) are never read by the MMA, and the zero rows after each
+    // record keep every read inside the slabs (a window ends at least one
+    // row before its slab does).
+    const int np = tc_panels(fb);
+    cuuint64_t dims[3] = {64, (cuuint64_t)rows, (cuuint64_t)np};
+    cuuint64_t strides[2] = {(cuuint64_t)(4 * fb), 128};
+    cuuint32_t box[3] = {64, 16, (cuuint32_t)np};
+    cuuint32_t es[3] = {1, 1, 1};
+    const CUresult cr = enc(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(job.S), dims, strides, box,
                             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;

@@ -63,7 +63,11 @@ constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
 constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
 constexpr int TC_NSB = 12;                 // window stages in shared memory
-constexpr int TC_PANEL_BYTES = TC_KCH * 2048;   // one 64-element panel of B: TC_KCH x (16 rows x 128 B)
+// A stage holds TC_KCH chunks of 16 window rows; a chunk is tc_panels(fb)
+// 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
+// swizzle), loaded by one 3-D TMA (x = element in the panel, y = row,
+// z = panel); the MMA's leading offset is the 2048-byte panel step.
+constexpr int TC_PANEL_BYTES = 2048;
 constexpr float TC_SCALE = 256.0f;
 constexpr RCABF_HD int tc_nmat(bool split) { return split ? 4 : 2; }
 constexpr RCABF_HD int tc_n16(int fb) { return (2 * fb + 15) / 16 * 16; }
@@ -73,7 +77,7 @@ constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return 2 * tc_n16(fb) 
 // largest frame block that fits the 512 columns
 constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 80 : 104; }
 // dynamic shared memory: TC_NSB stages of B panels + 1 KB for the 1024-byte alignment
-constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * TC_KCH * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
 
 // All lanes wait on the barrier; the warp proceeds (converged) only if every
 // lane saw the phase complete.
@@ -178,7 +182,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const int NH = 2 * FB;                 // halfs per slab row = MMA N
     const int N16 = tc_n16(FB);
     const int NP = tc_panels(FB);
-    const int stage_bytes = NP * TC_PANEL_BYTES;
+    const int chunk_bytes = NP * TC_PANEL_BYTES;
+    const int stage_bytes = TC_KCH * chunk_bytes;
     const int a_col0 = 2 * N16;            // first weight-matrix column
     const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
 
@@ -186,6 +191,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], empty_a[TC_NSA];
     __shared__ uint64_t acc_full, acc_empty, fin;
     __shared__ TcInfo info[TC_NSB];
+    __shared__ int2 win[32];   // producer: window (lo, nk) of each of 32 steps, nk = 0 when inactive
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
     uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -235,65 +241,64 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
 #pragma unroll
         for (int i = 0; i < TC_NSB; ++i) last_q[i] = -1;
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
-        bool stop = false;   // warp-uniform
-        // one record into the ring (lane 0 writes; the warp learns whether it could)
+        // lane 0 writes the records; the other lanes compute the windows of
+        // the next 32 steps with it.  stop: lane 0 could not (abort)
+        bool stop = false;
         auto emit = [&](const TcInfo rec, int64_t row0) {
-            int okw = 1;
-            if (lane == 0) {
-                const int st = (int)(q % TC_NSB);
-                okw = mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort) ? 1 : 0;
-                if (okw) {
-                    info[st] = rec;
-                    if (rec.kind == TC_STEP) {
-                        mbar_arrive_expect_tx(&full_b[st], (uint32_t)(rec.nk * NP * 2048));
-                        uint8_t *dst = Bs + st * stage_bytes;
-                        for (int j = 0; j < rec.nk; ++j)
-                            for (int p = 0; p < NP; ++p)
-                                tma_load_2d(dst + p * TC_PANEL_BYTES + j * 2048, &prm.tmap, &full_b[st], 64 * p,
-                                            (int32_t)(row0 + 16 * j));
-                        last_q[st] = (int)q;
-                    } else {
-                        mbar_arrive(&full_b[st]);
-                        last_q[st] = -1;   // no copy in flight
-                    }
-                }
+            const int st = (int)(q % TC_NSB);
+            if (!mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort)) { stop = true; return; }
+            info[st] = rec;
+            if (rec.kind == TC_STEP) {
+                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(rec.nk * chunk_bytes));
+                uint8_t *dst = Bs + st * stage_bytes;
+                for (int j = 0; j < rec.nk; ++j)
+                    tma_load_3d(dst + j * chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(row0 + 16 * j), 0);
+                last_q[st] = (int)q;
+            } else {
+                mbar_arrive(&full_b[st]);
+                last_q[st] = -1;   // no copy in flight
             }
-            okw = __shfl_sync(0xffffffffu, okw, 0);
             ++q;
-            if (!okw) stop = true;
         };
         int it = 0;
-        for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x, ++it) {
+        for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x, ++it) {
             const int fb = (int)(item / n_tiles);
             const int64_t tile = item % n_tiles;
             const int tz = (int)(tile % J.tiles_z);
             const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
             const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
             int n_active = 0;
-            for (int s0 = 0; s0 < n_steps && !stop; s0 += 32) {
+            for (int s0 = 0; s0 < n_steps; s0 += 32) {
                 const int s = s0 + lane;
                 int lo = 0, nk = 0;
-                bool act = false, ovf = false;
+                bool ovf = false;
                 if (s < n_steps) {
                     const int tx = s / g.n_ele, rx = s - tx * g.n_ele;
-                    act = tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf);
+                    if (!tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf)) nk = 0;
                     if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
                 }
-                unsigned mask = __ballot_sync(0xffffffffu, act);
-                while (mask && !stop) {
-                    const int i = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const int lo_i = __shfl_sync(0xffffffffu, lo, i);
-                    const int nk_i = __shfl_sync(0xffffffffu, nk, i);
-                    const int64_t row0 = ((int64_t)(s0 + i) * J.n_fb + fb) * prm.rows_per_slab + lo_i;
-                    const int tx_i = (s0 + i) / g.n_ele;
-                    emit(TcInfo{TC_STEP, s0 + i, lo_i, nk_i, it, 0, tx_i, s0 + i - tx_i * g.n_ele}, row0);
-                    ++n_active;
+                __syncwarp();
+                win[lane] = make_int2(lo, nk);
+                __syncwarp();
+                if (lane == 0) {
+                    for (int i = 0; i < 32 && s0 + i < n_steps && !stop; ++i) {
+                        const int2 wi = win[i];
+                        if (wi.y == 0) continue;
+                        const int si = s0 + i;
+                        const int64_t row0 = ((int64_t)si * J.n_fb + fb) * prm.rows_per_slab + wi.x;
+                        const int tx_i = si / g.n_ele;
+                        emit(TcInfo{TC_STEP, si, wi.x, wi.y, it, 0, tx_i, si - tx_i * g.n_ele}, row0);
+                        ++n_active;
+                    }
                 }
+                if (__shfl_sync(0xffffffffu, (int)stop, 0)) break;
             }
-            if (!stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
+            if (lane == 0 && !stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
+            if (__shfl_sync(0xffffffffu, (int)stop, 0)) break;
         }
-        for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
+        if (lane == 0)
+            for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
+        stop = __shfl_sync(0xffffffffu, (int)stop, 0) != 0;
         if (lane == 0 && stop) {
             // let the copies in flight land before the CTA's shared memory goes
             for (int st = 0; st < TC_NSB; ++st)
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 const uint32_t bbase = smem_u32(Bs + bst * stage_bytes);
                 const uint32_t acol = (uint32_t)(a_col0 + ast * NMAT * 16);
                 for (int j = 0; j < inf.nk; ++j) {
-                    const uint64_t bd = sdesc_mn_sw128(bbase + j * 2048, TC_PANEL_BYTES, 1024);
+                    const uint64_t bd = sdesc_mn_sw128(bbase + j * chunk_bytes, TC_PANEL_BYTES, 1024);
 #pragma unroll
                     for (int mat = 0; mat < NMAT; ++mat) {
                         const bool re = mat < NMAT / 2;

@@ -103,6 +103,17 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const void *tmap, uint64_
         : "memory");
 }
 
+// 3-D tile load, coordinates (x, y, z) innermost first
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, uint64_t *bar, int32_t x, int32_t y,
+                                            int32_t z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
 // ------------------------------------------------------------------------
 // tcgen05: MMA, commit, tensor-memory stores
 // ------------------------------------------------------------------------
