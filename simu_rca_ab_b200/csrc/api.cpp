@@ -167,7 +167,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
         size_t off = 0;
         p.off_S = off;
-        off += al((size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes);
+        // (tensor-core plans: the slabs, then right after them the same
+        // slabs holding (-im, re), one row range of the kernel's tensor map)
+        off += al((size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes * (p.tc ? 2 : 1));
         p.off_rxr = off;
         off += al((size_t)g->n_ele * p.tiles_u * p.tiles_z * sizeof(float2));
         p.off_txr = off;
@@ -222,7 +224,7 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
             p.ts = tts;
             p.tc_rows = (int)a->n_sample + TC_MAX_ROWS;
             layout(tts.tv);
-            ok = (int64_t)g->n_tx * g->n_ele * p.n_fb * p.tc_rows < ((int64_t)1 << 31);
+            ok = 2 * (int64_t)g->n_tx * g->n_ele * p.n_fb * p.tc_rows < ((int64_t)1 << 31);
         }
         if (ok) {
             p.wmax = TC_MAX_ROWS;
@@ -327,6 +329,7 @@ int stage_job(rcabf_geometry *g, const rcabf_beamform_args *a, const Plan &p, Fu
     ip.iq = a->iq; ip.iq_dtype = a->iq_dtype; ip.n_sample = (int)a->n_sample; ip.n_ele = g->n_ele;
     ip.n_tx = g->n_tx; ip.n_frame = a->n_frame; ip.fb = p.fb; ip.n_fb = p.n_fb;
     ip.S = ws + p.off_S; ip.slab_bytes = p.slab_bytes; ip.n_rows = p.tc ? p.tc_rows : 0;
+    ip.S2 = p.tc ? ws + p.off_S + (size_t)g->n_tx * g->n_ele * p.n_fb * p.slab_bytes : nullptr;
     cudaError_t ce = launch_ingest(ip, p.store, st);
     if (ce != cudaSuccess) return cuda_fail(ce, "ingest launch");
     if (marks) mark(marks, 1, st);
@@ -676,7 +679,7 @@ int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, c
         const int64_t chunks = const_cast<rcabf_geometry *>(g)->tc_chunks(p.ts, a->n_sample);
         const int nmat = p.tc == 2 ? 4 : 2;
         const int n16 = (2 * p.fb + 15) / 16 * 16;
-        mma_flops = (double)chunks * p.n_fb * nmat * 2.0 * 128.0 * n16 * 16.0;
+        mma_flops = (double)chunks * p.n_fb * nmat * 2.0 * 128.0 * n16 * 16.0;   // nmat MMAs per chunk
     }
     snprintf(buf, len,
              "{\"kernel\": \"%s\", \"row_shift\": %d, \"frames_per_block\": %d, \"frame_blocks\": %d, "

@@ -54,10 +54,17 @@ __global__ void __launch_bounds__(256) ingest_kernel(const IngestParams p)
     T *slab = reinterpret_cast<T *>(reinterpret_cast<char *>(p.S) +
                                     (((int64_t)tx * p.n_ele + ele) * p.n_fb + fb) * p.slab_bytes);
     const int n_rows = max(p.n_rows, p.n_sample);
+    T *slab2 = p.S2 == nullptr ? nullptr
+                               : reinterpret_cast<T *>(reinterpret_cast<char *>(p.S2) +
+                                                       (((int64_t)tx * p.n_ele + ele) * p.n_fb + fb) * p.slab_bytes);
     for (int i = threadIdx.x; i < FC * INGEST_NS; i += blockDim.x) {
         const int nl = i / FC, fi = i % FC;
         const int n = n_base + nl;
-        if (n < n_rows) slab[(int64_t)n * FB + f0 + fi] = from_f2<STORE>(tile[fi][nl]);   // zeros past the record
+        if (n < n_rows) {
+            const float2 v = tile[fi][nl];
+            slab[(int64_t)n * FB + f0 + fi] = from_f2<STORE>(v);   // zeros past the record
+            if (slab2) slab2[(int64_t)n * FB + f0 + fi] = from_f2<STORE>(make_float2(-v.y, v.x));
+        }
     }
 }
 

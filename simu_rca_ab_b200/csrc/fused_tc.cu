@@ -70,17 +70,19 @@ cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, in
 {
     if (fb < 32 || fb > tc_max_fb(split != 0) || (fb & 7) || tc_tmem_cols(fb, split != 0) > 512)
         return cudaErrorInvalidValue;
-    const int64_t rows = (int64_t)job.g.n_tx * job.g.n_ele * job.n_fb * rows_per_slab;
-    if (rows >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
+    const int64_t rows = (int64_t)job.g.n_tx * job.g.n_ele * job.n_fb * rows_per_slab;   // of each slab set
+    if (2 * rows >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
     auto enc = tensor_map_encoder();
     if (!enc) return cudaErrorNotSupported;
     TcParams p{};
     p.job = job;
     p.fb = fb;
     p.rows_per_slab = rows_per_slab;
+    p.s2_row0 = rows;
     p.n_items = n_items;
     p.err_count = err;
-    // the slabs as a 3-D FP16 tensor: x = element within a 64-element
+    // the two slab sets (samples, then (-im, re)) as one 3-D FP16 tensor:
+    // x = element within a 64-element
     // panel of a row (2-byte stride), y = row (rows of 2 fb halfs), z = panel
     // (128-byte stride); one box = one 16-row chunk of every panel, laid out
     // panel after panel with the 128-byte swizzle (the MMA's B layout).  The
@@ -89,7 +91,7 @@ cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, in
     // record keep every read inside the slabs (a window ends at least one
     // row before its slab does).
     const int np = tc_panels(fb);
-    cuuint64_t dims[3] = {64, (cuuint64_t)rows, (cuuint64_t)np};
+    cuuint64_t dims[3] = {64, (cuuint64_t)(2 * rows), (cuuint64_t)np};
     cuuint64_t strides[2] = {(cuuint64_t)(4 * fb), 128};
     cuuint32_t box[3] = {64, 16, (cuuint32_t)np};
     cuuint32_t es[3] = {1, 1, 1};

@@ -12,10 +12,11 @@
 //     out[m][f] += sum_k W[m][k] * S[lo + k][f],
 // and summing over all (tx, rx) steps is one long contraction: the tile's
 // accumulators stay in tensor memory across the whole acquisition.  S rows
-// hold the frames of a block as (re, im) FP16 pairs, so with the real and
-// imaginary parts of W in two matrices,
-//     D_r = Re(W) . S,  D_i = Im(W) . S    (N = 2 FB columns, (re, im) per frame)
-//     out_re = D_r[re] - D_i[im],  out_im = D_r[im] + D_i[re].
+// hold the frames of a block as (re, im) FP16 pairs, and the ingest writes a
+// second copy S' of the slabs holding (-im, re), so with the real and
+// imaginary parts of W in two matrices one accumulator takes both:
+//     D = Re(W) . S + Im(W) . S'    (N = 2 FB columns, (re, im) per frame)
+// i.e. D[re] = Re(W) S_re - Im(W) S_im, D[im] = Re(W) S_im + Im(W) S_re.
 // Weights are formed in FP32 exactly as the SIMT kernels form them (degree-6
 // polynomials, FP32 phasors) and enter the MMA as FP16: SPLIT = true adds a
 // second FP16 term holding the remainder (hi + lo carries ~22 bits, the MMA
@@ -42,9 +43,9 @@
 // is bounded (mbar_wait): a wait that runs out sets an abort flag, counts an
 // error and every role leaves its loop.
 //
-// Tensor memory (512 columns, one CTA per SM): D_r at column 0, D_i at
-// column N16, then TC_NSA slots of NMAT weight matrices of 16 columns (32
-// FP16 per row: K <= 32).
+// Tensor memory (512 columns, one CTA per SM): D at column 0 (N16 <= 256
+// columns), then TC_NSA slots of NMAT weight matrices of 16 columns (32 FP16
+// per row: K <= 32).
 #pragma once
 
 #include <cuda.h>
@@ -62,8 +63,9 @@ constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
 constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
 constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
-constexpr int TC_NSB = 12;                 // window stages in shared memory
-// A stage holds TC_KCH chunks of 16 window rows; a chunk is tc_panels(fb)
+constexpr int TC_NSB = 6;                  // window stages in shared memory
+// A stage holds the window of S and of S', each TC_KCH chunks of 16 rows; a
+// chunk is tc_panels(fb)
 // 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
 // swizzle), loaded by one 3-D TMA (x = element in the panel, y = row,
 // z = panel); the MMA's leading offset is the 2048-byte panel step.
@@ -73,11 +75,11 @@ constexpr RCABF_HD int tc_nmat(bool split) { return split ? 4 : 2; }
 constexpr RCABF_HD int tc_n16(int fb) { return (2 * fb + 15) / 16 * 16; }
 constexpr RCABF_HD int tc_panels(int fb) { return (2 * fb + 63) / 64; }
 // tensor-memory columns the kernel needs at frame block fb
-constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return 2 * tc_n16(fb) + TC_NSA * (split ? 4 : 2) * 16; }
-// largest frame block that fits the 512 columns
-constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 80 : 104; }
+constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return tc_n16(fb) + TC_NSA * (split ? 4 : 2) * 16; }
+// largest frame block: the MMA's N = 2 FB is at most 256
+constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 128 : 128; }
 // dynamic shared memory: TC_NSB stages of B panels + 1 KB for the 1024-byte alignment
-constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * TC_KCH * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * 2 * TC_KCH * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
 
 // All lanes wait on the barrier; the warp proceeds (converged) only if every
 // lane saw the phase complete.
@@ -108,6 +110,7 @@ struct TcParams {
     FusedJob job;
     int32_t fb;                 // frames per block (multiple of 8, 32..tc_max_fb)
     int32_t rows_per_slab;      // n_sample + 32 (zero rows past the record)
+    int64_t s2_row0;            // first row of the (-im, re) slabs S' in the tensor map
     int64_t n_items;            // n_fb * tiles
     unsigned long long *err_count;
 };
@@ -183,8 +186,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const int N16 = tc_n16(FB);
     const int NP = tc_panels(FB);
     const int chunk_bytes = NP * TC_PANEL_BYTES;
-    const int stage_bytes = TC_KCH * chunk_bytes;
-    const int a_col0 = 2 * N16;            // first weight-matrix column
+    const int half_bytes = TC_KCH * chunk_bytes;   // the S window; the S' window follows
+    const int stage_bytes = 2 * half_bytes;
+    const int a_col0 = N16;                // first weight-matrix column
     const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
 
     extern __shared__ uint8_t smem_raw[];
@@ -249,10 +253,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             if (!mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort)) { stop = true; return; }
             info[st] = rec;
             if (rec.kind == TC_STEP) {
-                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(rec.nk * chunk_bytes));
+                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * rec.nk * chunk_bytes));
                 uint8_t *dst = Bs + st * stage_bytes;
-                for (int j = 0; j < rec.nk; ++j)
+                for (int j = 0; j < rec.nk; ++j) {
                     tma_load_3d(dst + j * chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(row0 + 16 * j), 0);
+                    tma_load_3d(dst + half_bytes + j * chunk_bytes, &prm.tmap, &full_b[st], 0,
+                                (int32_t)(prm.s2_row0 + row0 + 16 * j), 0);
+                }
                 last_q[st] = (int)q;
             } else {
                 mbar_arrive(&full_b[st]);
@@ -311,7 +318,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             uint32_t q = 0;
-            bool issued = false, first = true, dr = false, di = false;
+            bool issued = false, first = true, dacc = false;
             for (;;) {
                 const int bst = (int)(q % TC_NSB);
                 if (!mbar_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
@@ -332,20 +339,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     mbar_arrive(&empty_a[ast]);
                     mbar_arrive(&empty_b[bst]);
                     first = true;
-                    dr = di = false;
+                    dacc = false;
                     continue;
                 }
                 tmem_fence_after_sync();
                 const uint32_t bbase = smem_u32(Bs + bst * stage_bytes);
                 const uint32_t acol = (uint32_t)(a_col0 + ast * NMAT * 16);
                 for (int j = 0; j < inf.nk; ++j) {
-                    const uint64_t bd = sdesc_mn_sw128(bbase + j * chunk_bytes, TC_PANEL_BYTES, 1024);
+                    const uint64_t bs = sdesc_mn_sw128(bbase + j * chunk_bytes, TC_PANEL_BYTES, 1024);
+                    const uint64_t bs2 = sdesc_mn_sw128(bbase + half_bytes + j * chunk_bytes, TC_PANEL_BYTES, 1024);
 #pragma unroll
                     for (int mat = 0; mat < NMAT; ++mat) {
-                        const bool re = mat < NMAT / 2;
-                        const uint32_t d = tb + (re ? 0u : (uint32_t)N16);
-                        umma_f16_ts(d, tb + acol + mat * 16 + 8 * j, bd, idesc, (re ? dr : di) ? 1u : 0u);
-                        if (re) dr = true; else di = true;
+                        // Re(W) against S, Im(W) against S' = (-im, re)
+                        umma_f16_ts(tb, tb + acol + mat * 16 + 8 * j, mat < NMAT / 2 ? bs : bs2, idesc, dacc ? 1u : 0u);
+                        dacc = true;
                     }
                 }
                 umma_commit(&empty_b[bst]);
@@ -395,16 +402,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             if (inf.kind == TC_END) {
                 if (!warp_wait(&empty_a[ast], a_par, abort)) break;
                 mbar_arrive(&full_a[ast]);
-                // ---- epilogue: D_r, D_i -> out (frames of this block) ----
+                // ---- epilogue: D -> out (frames of this block) ----
                 if (!warp_wait(&acc_full, (uint32_t)inf.it & 1u, abort)) break;
                 tmem_fence_after_sync();
                 const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
                 for (int c = 0; c < N16; c += 16) {
-                    uint32_t r[16], i16[16];
+                    uint32_t r[16];
                     tmem_ld16(lane_base + (uint32_t)c, r);
-                    tmem_ld16(lane_base + (uint32_t)(N16 + c), i16);
                     tmem_wait_ld16(r);
-                    tmem_wait_ld16(i16);
                     if (valid) {
 #pragma unroll
                         for (int h = 0; h < 8; ++h) {
@@ -412,10 +417,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                             if (c / 2 + h < FB && f < J.n_frame) {
                                 float2 val = make_float2(0.f, 0.f);
                                 if (inf.n > 0) {
-                                    val.x = (__uint_as_float(r[2 * h]) - __uint_as_float(i16[2 * h + 1])) *
-                                            (1.0f / TC_SCALE);
-                                    val.y = (__uint_as_float(r[2 * h + 1]) + __uint_as_float(i16[2 * h])) *
-                                            (1.0f / TC_SCALE);
+                                    val.x = __uint_as_float(r[2 * h]) * (1.0f / TC_SCALE);
+                                    val.y = __uint_as_float(r[2 * h + 1]) * (1.0f / TC_SCALE);
                                 }
                                 float2 *op = J.out + (int64_t)f * g.n_pix + pix;
                                 if (J.accumulate) { float2 x = *op; x.x += val.x; x.y += val.y; *op = x; }

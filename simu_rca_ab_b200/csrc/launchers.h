@@ -16,6 +16,7 @@ struct IngestParams {
     void *S;
     int64_t slab_bytes;
     int32_t n_rows;        // rows written per slab: n_sample, or more with zero rows past the record
+    void *S2;              // NULL, or a second slab set of the same layout holding (-im, re)
 };
 
 struct RangeParams {

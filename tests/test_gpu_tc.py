@@ -95,11 +95,11 @@ def test_tensor_core_kernel_vs_fp64_and_simt_on_the_ensemble_geometry(c2_40, kna
     assert np.isfinite(o).all()
 
 
-@pytest.mark.parametrize("kname,n_frame", [("tc", 100), ("tc16", 100), ("tc", 33)])
+@pytest.mark.parametrize("kname,n_frame", [("tc", 100), ("tc16", 100), ("tc", 33), ("tc", 300)])
 def test_frame_blocks_and_padding(cuda, kname, n_frame):
-    """Several frame blocks (100 frames: two blocks of 56 hi + remainder, one of
-    104 single) and a block padded from 33 to 40 frames give every frame the
-    SIMT kernel's value."""
+    """One block of 104 frames for 100 frames (either weight precision) and a
+    block padded from 33 to 40 frames give every frame the SIMT kernel's
+    value."""
     from simu_rca_ab_b200 import _lib as L
     from simu_rca_ab_b200 import workloads as W
     w = W.get("c2", n_frame=n_frame)
