@@ -30,8 +30,9 @@
 // q mod 3 = g, so that the groups' dependent setup chains overlap), and the
 // group that
 // meets an item's end record writes that item's outputs; warp 12 computes
-// the windows of 32 steps at a time and loads each active step's window with
-// 2-D TMA (128-byte swizzle) into a ring of TC_NSB shared-memory stages, up
+// the windows of 32 steps at a time; each of its lanes with an active step
+// writes that step's record and loads its window with 3-D TMA (128-byte
+// swizzle) into its own stage of a ring of TC_NSB shared-memory stages, up
 // to TC_NSB records ahead of the MMAs, so the load latency stays off the
 // critical path; warp 13 issues the MMAs (A from one of TC_NSA tensor-memory
 // weight slots, B from shared memory) and commits them to the slot's and
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], empty_a[TC_NSA];
     __shared__ uint64_t acc_full, acc_empty, fin;
     __shared__ TcInfo info[TC_NSB];
-    __shared__ int2 win[32];   // producer: window (lo, nk) of each of 32 steps, nk = 0 when inactive
+    __shared__ volatile int last_rec[TC_NSB];   // producer: latest record loaded into each stage, -1 none
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
     uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -219,6 +220,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             mbar_init(&full_a[i], 128);
             mbar_init(&empty_a[i], 1);
         }
+        for (int i = 0; i < TC_NSB; ++i) last_rec[i] = -1;
         mbar_init(&acc_full, 1);
         mbar_init(&acc_empty, 128);
         mbar_init(&fin, 1);
@@ -240,19 +242,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
 
     if (warp == TC_PRODUCER_WARP) {
         // ---------------- producer: windows and TMA loads ----------------
-        uint32_t q = 0;
-        int last_q[TC_NSB];
-#pragma unroll
-        for (int i = 0; i < TC_NSB; ++i) last_q[i] = -1;
+        // The warp computes the windows of 32 steps at a time; each lane with
+        // an active step then writes that step's record itself (its place in
+        // the ring is the step's rank among the active ones), so up to
+        // TC_NSB records are written and loaded at once, each lane waiting on
+        // its own stage.
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
-        // lane 0 writes the records; the other lanes compute the windows of
-        // the next 32 steps with it.  stop: lane 0 could not (abort)
-        bool stop = false;
-        auto emit = [&](const TcInfo rec, int64_t row0) {
-            const int st = (int)(q % TC_NSB);
-            if (!mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort)) { stop = true; return; }
+        uint32_t q = 0;          // next record (warp-uniform)
+        bool stop = false;       // warp-uniform after each batch
+        auto emit = [&](uint32_t qr, const TcInfo rec, int64_t row0) -> bool {
+            const int st = (int)(qr % TC_NSB);
+            if (!mbar_wait(&empty_b[st], ((qr / TC_NSB) & 1u) ^ 1u, abort)) return false;
             info[st] = rec;
             if (rec.kind == TC_STEP) {
+                last_rec[st] = (int)qr;
                 mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * rec.nk * chunk_bytes));
                 uint8_t *dst = Bs + st * stage_bytes;
                 for (int j = 0; j < rec.nk; ++j) {
@@ -260,58 +263,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     tma_load_3d(dst + half_bytes + j * chunk_bytes, &prm.tmap, &full_b[st], 0,
                                 (int32_t)(prm.s2_row0 + row0 + 16 * j), 0);
                 }
-                last_q[st] = (int)q;
             } else {
+                last_rec[st] = -1;   // no copy in flight
                 mbar_arrive(&full_b[st]);
-                last_q[st] = -1;   // no copy in flight
             }
-            ++q;
+            return true;
         };
         int it = 0;
-        for (int64_t item = blockIdx.x; item < prm.n_items; item += gridDim.x, ++it) {
+        for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x, ++it) {
             const int fb = (int)(item / n_tiles);
             const int64_t tile = item % n_tiles;
             const int tz = (int)(tile % J.tiles_z);
             const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
             const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
             int n_active = 0;
-            for (int s0 = 0; s0 < n_steps; s0 += 32) {
+            for (int s0 = 0; s0 < n_steps && !stop; s0 += 32) {
                 const int s = s0 + lane;
-                int lo = 0, nk = 0;
-                bool ovf = false;
+                int lo = 0, nk = 0, tx = 0, rx = 0;
+                bool act = false, ovf = false;
                 if (s < n_steps) {
-                    const int tx = s / g.n_ele, rx = s - tx * g.n_ele;
-                    if (!tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf)) nk = 0;
+                    tx = s / g.n_ele;
+                    rx = s - tx * g.n_ele;
+                    act = tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf);
                     if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
                 }
-                __syncwarp();
-                win[lane] = make_int2(lo, nk);
-                __syncwarp();
-                if (lane == 0) {
-                    for (int i = 0; i < 32 && s0 + i < n_steps && !stop; ++i) {
-                        const int2 wi = win[i];
-                        if (wi.y == 0) continue;
-                        const int si = s0 + i;
-                        const int64_t row0 = ((int64_t)si * J.n_fb + fb) * prm.rows_per_slab + wi.x;
-                        const int tx_i = si / g.n_ele;
-                        emit(TcInfo{TC_STEP, si, wi.x, wi.y, it, 0, tx_i, si - tx_i * g.n_ele}, row0);
-                        ++n_active;
-                    }
+                const unsigned mask = __ballot_sync(0xffffffffu, act);
+                bool ok = true;
+                if (act) {
+                    const uint32_t qr = q + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+                    const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo;
+                    ok = emit(qr, TcInfo{TC_STEP, s, lo, nk, it, 0, tx, rx}, row0);
                 }
-                if (__shfl_sync(0xffffffffu, (int)stop, 0)) break;
+                stop = __any_sync(0xffffffffu, !ok);
+                q += (uint32_t)__popc(mask);
+                n_active += __popc(mask);
             }
-            if (lane == 0 && !stop) emit(TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
-            if (__shfl_sync(0xffffffffu, (int)stop, 0)) break;
+            if (!stop) {   // end of item
+                bool ok = true;
+                if (lane == 0) ok = emit(q, TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
+                stop = __any_sync(0xffffffffu, !ok);
+                ++q;
+            }
         }
-        if (lane == 0)
-            for (int k = 0; k < TC_GROUPS && !stop; ++k) emit(TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
-        stop = __shfl_sync(0xffffffffu, (int)stop, 0) != 0;
+        if (!stop) {   // one final record per builder group
+            bool ok = true;
+            if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
+            stop = __any_sync(0xffffffffu, !ok);
+        }
         if (lane == 0 && stop) {
             // let the copies in flight land before the CTA's shared memory goes
             for (int st = 0; st < TC_NSB; ++st)
-                if (last_q[st] >= 0) {
+                if (last_rec[st] >= 0) {
                     volatile int dummy = 0;
-                    mbar_wait(&full_b[st], ((uint32_t)last_q[st] / TC_NSB) & 1u, &dummy, 100000000ull);
+                    mbar_wait(&full_b[st], ((uint32_t)last_rec[st] / TC_NSB) & 1u, &dummy, 100000000ull);
                 }
         }
     } else if (warp == TC_MMA_WARP) {
