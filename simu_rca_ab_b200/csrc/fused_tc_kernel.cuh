@@ -65,6 +65,7 @@ constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
 constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
 constexpr int TC_NSB = 6;                  // window stages in shared memory
+static_assert(TC_GROUPS <= TC_NSB, "the final records are written in one round");
 // A stage holds the window of S and of S', each TC_KCH chunks of 16 rows; a
 // chunk is tc_panels(fb)
 // 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
@@ -244,9 +245,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         // ---------------- producer: windows and TMA loads ----------------
         // The warp computes the windows of 32 steps at a time; each lane with
         // an active step then writes that step's record itself (its place in
-        // the ring is the step's rank among the active ones), so up to
-        // TC_NSB records are written and loaded at once, each lane waiting on
-        // its own stage.
+        // the ring is the step's rank among the active ones), TC_NSB lanes at
+        // a time, each lane waiting on its own stage.
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
         uint32_t q = 0;          // next record (warp-uniform)
         bool stop = false;       // warp-uniform after each batch
@@ -288,15 +288,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
                 }
                 const unsigned mask = __ballot_sync(0xffffffffu, act);
-                bool ok = true;
-                if (act) {
-                    const uint32_t qr = q + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-                    const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo;
-                    ok = emit(qr, TcInfo{TC_STEP, s, lo, nk, it, 0, tx, rx}, row0);
+                const int n_act = __popc(mask);
+                const int rank = __popc(mask & ((1u << lane) - 1u));
+                // in rounds of at most TC_NSB records: a stage's barrier
+                // tells apart only the phase of its previous use, so no lane
+                // may wait on a stage more than one use ahead of the records
+                // already written
+                for (int r0 = 0; r0 < n_act && !stop; r0 += TC_NSB) {
+                    bool ok = true;
+                    if (act && rank >= r0 && rank < r0 + TC_NSB) {
+                        const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo;
+                        ok = emit(q + (uint32_t)rank, TcInfo{TC_STEP, s, lo, nk, it, 0, tx, rx}, row0);
+                    }
+                    stop = __any_sync(0xffffffffu, !ok);
                 }
-                stop = __any_sync(0xffffffffu, !ok);
-                q += (uint32_t)__popc(mask);
-                n_active += __popc(mask);
+                q += (uint32_t)n_act;
+                n_active += n_act;
             }
             if (!stop) {   // end of item
                 bool ok = true;
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 ++q;
             }
         }
-        if (!stop) {   // one final record per builder group
+        if (!stop) {   // one final record per builder group (TC_GROUPS <= TC_NSB)
             bool ok = true;
             if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
             stop = __any_sync(0xffffffffu, !ok);
