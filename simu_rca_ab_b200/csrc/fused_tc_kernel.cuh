@@ -35,8 +35,8 @@
 // swizzle) into its own stage of a ring of TC_NSB shared-memory stages, up
 // to TC_NSB records ahead of the MMAs, so the load latency stays off the
 // critical path; warp 13 issues the MMAs (A from one of TC_NSA tensor-memory
-// weight slots, B from shared memory) and commits them to the slot's and
-// the stage's "empty" barriers.  Steps whose window is empty for the whole
+// weight slots, B from shared memory) and commits them to the stage's
+// "empty" barrier, which also tells the builders the slot is free.  Steps whose window is empty for the whole
 // tile are skipped by every role alike: the producer passes each active
 // step's record (step, window start, 16-row chunks, item) through the stage
 // ring, then an end-of-item record (with the item's count of active steps),
@@ -63,9 +63,10 @@ constexpr int TC_GROUPS = 3;               // builder groups of 4 warps
 constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
 constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
-constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory
+constexpr int TC_NSA = TC_GROUPS;          // weight-matrix slots in tensor memory: group g uses slot g
 constexpr int TC_NSB = 6;                  // window stages in shared memory
 static_assert(TC_GROUPS <= TC_NSB, "the final records are written in one round");
+static_assert(TC_NSB > TC_NSA, "slot reuse is signalled through the window stages");
 // A stage holds the window of S and of S', each TC_KCH chunks of 16 rows; a
 // chunk is tc_panels(fb)
 // 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
 
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], empty_a[TC_NSA];
+    __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA];
     __shared__ uint64_t acc_full, acc_empty, fin;
     __shared__ TcInfo info[TC_NSB];
     __shared__ volatile int last_rec[TC_NSB];   // producer: latest record loaded into each stage, -1 none
@@ -219,7 +220,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         }
         for (int i = 0; i < TC_NSA; ++i) {
             mbar_init(&full_a[i], 128);
-            mbar_init(&empty_a[i], 1);
         }
         for (int i = 0; i < TC_NSB; ++i) last_rec[i] = -1;
         mbar_init(&acc_full, 1);
@@ -347,7 +347,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 }
                 if (inf.kind == TC_END) {
                     umma_commit(&acc_full);
-                    mbar_arrive(&empty_a[ast]);
                     mbar_arrive(&empty_b[bst]);
                     first = true;
                     dacc = false;
@@ -366,8 +365,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                         dacc = true;
                     }
                 }
-                umma_commit(&empty_b[bst]);
-                umma_commit(&empty_a[ast]);
+                umma_commit(&empty_b[bst]);   // releases the stage and, for the builders, the weight slot
                 issued = true;
             }
             if (*abort && issued) {   // the MMAs in flight complete before the columns are freed
@@ -409,9 +407,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 pre_s = -1;
             }
             const int ast = (int)(q % TC_NSA);
-            const uint32_t a_par = ((q / TC_NSA) & 1u) ^ 1u;   // the slot's previous use has been consumed
+            // the slot's previous use, record q - TC_NSA (built by this group),
+            // has been consumed: its MMAs completed, which the MMA warp
+            // signals on the window stage that record used.  That stage's
+            // barrier is at most one use behind or ahead of the wait (this
+            // group built record q - 2 TC_NSA only after record q - 3 TC_NSA
+            // was consumed, and record q + TC_NSB - TC_NSA is built after
+            // this one), so its parity identifies the use.
+            auto wait_slot = [&]() -> bool {
+                if (q < (uint32_t)TC_NSA) return true;
+                const uint32_t qp = q - TC_NSA;
+                return warp_wait(&empty_b[qp % TC_NSB], (qp / TC_NSB) & 1u, abort);
+            };
             if (inf.kind == TC_END) {
-                if (!warp_wait(&empty_a[ast], a_par, abort)) break;
+                if (!wait_slot()) break;
                 mbar_arrive(&full_a[ast]);
                 // ---- epilogue: D -> out (frames of this block) ----
                 if (!warp_wait(&acc_full, (uint32_t)inf.it & 1u, abort)) break;
@@ -501,7 +510,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                         words[1][c] = tc_pack(ai, bi);
                     }
                 }
-                if (!warp_wait(&empty_a[ast], a_par, abort)) return false;
+                if (!wait_slot()) return false;
                 tmem_fence_after_sync();
 #pragma unroll
                 for (int mat = 0; mat < NMAT; ++mat)
