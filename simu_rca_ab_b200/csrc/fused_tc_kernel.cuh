@@ -38,9 +38,11 @@
 // weight slots, B from shared memory) and commits them to the stage's
 // "empty" barrier, which also tells the builders the slot is free.  Steps whose window is empty for the whole
 // tile are skipped by every role alike: the producer passes each active
-// step's record (step, window start, 16-row chunks, item) through the stage
-// ring, then an end-of-item record (with the item's count of active steps),
-// and after the last item one final record per builder group.  Every wait
+// step's record (step, window start, 16-row chunks, item) through a ring of
+// TC_NSR record slots -- the builders start on a record as soon as it is
+// written, ahead of its window's load -- then an end-of-item record (with
+// the item's count of active steps), and after the last item one final
+// record per builder group.  Every wait
 // is bounded (mbar_wait): a wait that runs out sets an abort flag, counts an
 // error and every role leaves its loop.
 //
@@ -67,6 +69,8 @@ constexpr int TC_NSA = TC_GROUPS;          // weight-matrix slots in tensor memo
 constexpr int TC_NSB = 6;                  // window stages in shared memory
 static_assert(TC_GROUPS <= TC_NSB, "the final records are written in one round");
 static_assert(TC_NSB > TC_NSA, "slot reuse is signalled through the window stages");
+constexpr int TC_NSR = 2 * TC_NSB;         // records in flight (a ring of its own, ahead of the window loads)
+static_assert(TC_NSR >= TC_NSB, "a record is written before its window is loaded");
 // A stage holds the window of S and of S', each TC_KCH chunks of 16 rows; a
 // chunk is tc_panels(fb)
 // 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
@@ -195,9 +199,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
 
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA];
+    __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], rec_full[TC_NSR], rec_empty[TC_NSR];
     __shared__ uint64_t acc_full, acc_empty, fin;
-    __shared__ TcInfo info[TC_NSB];
+    __shared__ TcInfo info[TC_NSR];
     __shared__ volatile int last_rec[TC_NSB];   // producer: latest record loaded into each stage, -1 none
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
@@ -217,6 +221,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         for (int i = 0; i < TC_NSB; ++i) {
             mbar_init(&full_b[i], 1);
             mbar_init(&empty_b[i], 1);
+        }
+        for (int i = 0; i < TC_NSR; ++i) {
+            mbar_init(&rec_full[i], 1);
+            mbar_init(&rec_empty[i], 1);
         }
         for (int i = 0; i < TC_NSA; ++i) {
             mbar_init(&full_a[i], 128);
@@ -250,10 +258,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
         uint32_t q = 0;          // next record (warp-uniform)
         bool stop = false;       // warp-uniform after each batch
+        // a record first goes into its record slot (free once the MMA warp
+        // is done with the record TC_NSR earlier), where the builders pick it
+        // up; its window is then loaded into its stage (free once the MMAs of
+        // the record TC_NSB earlier completed), which the MMA warp waits for
         auto emit = [&](uint32_t qr, const TcInfo rec, int64_t row0) -> bool {
+            const int rs = (int)(qr % TC_NSR);
+            if (!mbar_wait(&rec_empty[rs], ((qr / TC_NSR) & 1u) ^ 1u, abort)) return false;
+            info[rs] = rec;
+            mbar_arrive(&rec_full[rs]);
             const int st = (int)(qr % TC_NSB);
             if (!mbar_wait(&empty_b[st], ((qr / TC_NSB) & 1u) ^ 1u, abort)) return false;
-            info[st] = rec;
             if (rec.kind == TC_STEP) {
                 last_rec[st] = (int)qr;
                 mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * rec.nk * chunk_bytes));
@@ -331,10 +346,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             uint32_t q = 0;
             bool issued = false, first = true, dacc = false;
             for (;;) {
-                const int bst = (int)(q % TC_NSB);
-                if (!mbar_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
-                const TcInfo inf = read_info(&info[bst]);
+                const int bst = (int)(q % TC_NSB), rs = (int)(q % TC_NSR);
+                if (!mbar_wait(&rec_full[rs], (q / TC_NSR) & 1u, abort)) break;
+                const TcInfo inf = read_info(&info[rs]);
                 if (inf.kind == TC_FINAL) break;
+                if (!mbar_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
                 const int ast = (int)(q % TC_NSA);
                 if (!mbar_wait(&full_a[ast], (q / TC_NSA) & 1u, abort)) break;
                 ++q;
@@ -348,6 +364,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 if (inf.kind == TC_END) {
                     umma_commit(&acc_full);
                     mbar_arrive(&empty_b[bst]);
+                    mbar_arrive(&rec_empty[rs]);
                     first = true;
                     dacc = false;
                     continue;
@@ -366,6 +383,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     }
                 }
                 umma_commit(&empty_b[bst]);   // releases the stage and, for the builders, the weight slot
+                mbar_arrive(&rec_empty[rs]);
                 issued = true;
             }
             if (*abort && issued) {   // the MMAs in flight complete before the columns are freed
@@ -387,9 +405,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         float itx = 0.f, ptr = 0.f, pti = 0.f;
         float4 pre_e = make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t q = (uint32_t)grp;; q += TC_GROUPS) {
-            const int bst = (int)(q % TC_NSB);
-            if (!warp_wait(&full_b[bst], (q / TC_NSB) & 1u, abort)) break;
-            const TcInfo inf = read_info(&info[bst]);
+            const int rs = (int)(q % TC_NSR);
+            if (!warp_wait(&rec_full[rs], (q / TC_NSR) & 1u, abort)) break;
+            const TcInfo inf = read_info(&info[rs]);
             if (inf.kind == TC_FINAL) break;
             if (inf.it != cur_it) {   // a new item: this thread's voxel
                 cur_it = inf.it;
