@@ -387,6 +387,10 @@ def simulator_leg(dev, seed: int = 7):
             "note": "scatterers static within a frame: one element field per frame, all transmits as one GEMM"}
 
 
+WORKLOAD_KIND = {"c0": "single volume, 64+64 probe", "c1": "row + column transmits compounded, 128+128 probe",
+                 "c2": "Doppler ensemble", "c4": "large volume, 256+256 probe, row + column transmits"}
+
+
 def tensor_peak():
     """Dense FP16/BF16 tensor peak (TFLOP/s) and where it comes from: the
     pool's measured figure (sustained: the kernel runs inside a long step)
@@ -849,7 +853,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded point scatterers, -30 dB noise)",
-            "config": {"workload": f"{w.name}: Doppler ensemble, [{w.n_sample} x {w.n_ele} x {w.n_tx} x {F}] I/Q, "
+            "config": {"workload": f"{w.name}: {WORKLOAD_KIND.get(w.name, 'acquisition')}, "
+                                   f"[{w.n_sample} x {w.n_ele} x {w.n_tx} x {F}] I/Q, "
                                    f"grid {w.grid_shape[1]}x{w.grid_shape[2]}x{w.grid_shape[0]}, Lanczos a={w.lanczos_a}, "
                                    f"f-number {w.Param['fnumber']}",
                        "storage": storage, "kernel": a.kernel, "l2": "inputs larger than L2 (no flush needed)",
