@@ -229,8 +229,19 @@ def serving_leg(eng, dev, n_requests: int, rates, seed: int = 3, plain: bool = T
 
     def serve(items, kernel, budget):
         # the first launch of each kernel variant sets its shared-memory limit
-        # inside the stream, as it would in a live service
-        srv = Server(eng, budget, n_streams=4, max_queue=4 * n_requests, max_batch=24)
+        # inside the stream, as it would in a live service.  The arena is one
+        # allocation: step down from the budget until the device grants it
+        # (the stream's own buffers are allocated by now)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        while True:
+            try:
+                srv = Server(eng, budget, n_streams=4, max_queue=4 * n_requests, max_batch=24)
+                break
+            except L.RcabfError:
+                if budget < 16e9:
+                    raise
+                budget = int(budget * 0.9)
         tickets = []
         t0 = time.perf_counter()
         for r, g, iq, out, _ in items:
@@ -246,28 +257,20 @@ def serving_leg(eng, dev, n_requests: int, rates, seed: int = 3, plain: bool = T
         return {"p50_ms": st.p50_ms, "p95_ms": st.p95_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
                 "max_ms": st.max_ms, "value": st.units_done / st.span_s if st.span_s > 0 else None, "unit": UNIT,
                 "launches": st.launches, "requests": len(items), "busy_s": st.busy_s, "span_s": st.span_s,
-                "arena_peak_bytes": st.arena_peak_bytes}
+                "arena_peak_bytes": st.arena_peak_bytes, "hbm_budget_bytes": budget}
 
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(min(150e9, free - 8e9))
-    # the arena is one allocation: step down until the device grants it
-    while True:
-        try:
-            Server(eng, budget, n_streams=1, max_queue=1, max_batch=1).close()
-            break
-        except L.RcabfError:
-            if budget < 16e9:
-                raise
-            budget = int(budget * 0.9)
     res = {"workload": f"c3 serving mix: {n_requests} requests per stream, Poisson arrivals (seed {seed}); probe "
                        "64+64 or 128+128, 1-32 tx, 1-64 frames, grids 32x32x64..128x128x256, FP32/FP16 storage, "
                        "f-number 1.5, Lanczos a=3; channel data and geometry tables resident",
            "hbm_budget_bytes": budget,
            "hbm_budget_note": "150 GB as configured" if budget >= 150e9 else
-                              f"150 GB configured; {free / 1e9:.1f} GB free on the device; the largest arena the "
-                              f"device granted in one allocation, 8 GB kept back",
+                              f"150 GB configured; {free / 1e9:.1f} GB free on the device, 8 GB kept back; each "
+                              f"stream's arena is the largest the device then granted in one allocation "
+                              f"(hbm_budget_bytes per stream)",
            "rates": []}
     items0 = None
     for rate in sorted(rates):
@@ -406,6 +409,84 @@ def tensor_peak():
         except (ValueError, OSError):
             pass
     return 1590.0, "1.59 PFLOP/s dense bf16 burst, an earlier measurement on this pool (of fallback)"
+
+
+def int8_peak(dev):
+    """Dense int8 tensor throughput (TOP/s) measured live: cuBLASLt int8 GEMM
+    (torch._int_mm, 8192^3, 2 N^3 ops), best of 5 after warm-up."""
+    import torch
+    n = 8192
+    a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev)
+    b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev).t()
+    for _ in range(3):
+        torch._int_mm(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def clutter_leg(x, dev, reps: int = 5):
+    """The SVD clutter filter of the beamformed ensemble x ([frame][voxel]):
+    its Gram on the int8 tensor cores (rcabf_casorati_gram) against the FP64
+    cuBLAS ZGEMM Gram, the whole filter with each, on the device (CUDA events
+    on the current stream, median of ``reps`` after a warm-up)."""
+    import numpy as np
+    import torch
+    from simu_rca_ab_b200.clutter import casorati_gram, gram_plan, svd_clutter_filter
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    n_t, n_pix = x.shape
+    plan = gram_plan(n_t, n_pix)
+    ws = torch.empty(int(plan["workspace_bytes"]) + 256, dtype=torch.uint8, device=dev)
+    g_tc = casorati_gram(x, workspace=ws)
+    ms_tc = timed(lambda: casorati_gram(x, workspace=ws))
+    x64 = x.to(torch.complex128)
+    g64 = x64.conj() @ x64.T
+    ms_64 = timed(lambda: x.to(torch.complex128).conj() @ x.to(torch.complex128).T)
+    del x64
+    gerr = float((g_tc - g64).abs().max() / g64.abs().max())
+    del g_tc, g64
+    peak = int8_peak(dev)
+    tops = plan["mma_int_ops"] / (ms_tc * 1e-3) / 1e12
+    ms_f_tc = timed(lambda: svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C"))
+    ms_f_64 = timed(lambda: svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C", gram="fp64"))
+    xf, ev = svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C")
+    xr, _ = svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C", gram="fp64")
+    frel = float((xf - xr).abs().pow(2).sum().sqrt() / xr.abs().pow(2).sum().sqrt())
+    kept = float((xf.abs() ** 2).sum() / (x.abs() ** 2).sum())
+    del xf, xr, ws
+    return {"what": f"SVDClutterFilter high-pass w=0.1 on the beamformed ensemble ({n_pix} voxels x {n_t} "
+                    "frames): Gram on the int8 tensor cores (4 x 7-bit slices, exact int32 sums, FP64 "
+                    "levels and chunks), FP64 eigh, FP32 projection (CGEMM)",
+            "ms": ms_f_tc, "ms_with_fp64_zgemm_gram": ms_f_64, "energy_kept": kept,
+            "filtered_rel_vs_fp64_gram": frel,
+            "gram": {"ms": ms_tc, "ms_fp64_zgemm": ms_64, "speedup_vs_fp64_zgemm": ms_64 / ms_tc,
+                     "max_err_rel_max_fp64": gerr, "mma_int_ops": plan["mma_int_ops"],
+                     "int_tops": tops, "int8_peak_tops": peak,
+                     "int8_peak_source": "cuBLASLt int8 GEMM 8192^3 measured live (torch._int_mm)",
+                     "tensor_frac": tops / peak, "plan": plan,
+                     "note": "ms covers the 4 launches (slicing, MMA, chunk reduction, assembly); "
+                             "tensor_frac is the MMA work of the whole call over that time"}}
 
 
 def ref_gpu_leg(w, data, frames: int, variant: str = "fast"):
@@ -624,26 +705,13 @@ def main():
         except Exception as ex:   # reported in the line, the eager number stands
             graph = {"error": f"{type(ex).__name__}: {ex}"}
 
-    # the downstream SVD clutter filter on this ensemble (Gram in FP64,
-    # eigen-decomposition, projection), timed on the device
+    # the downstream SVD clutter filter on this ensemble: Gram on the int8
+    # tensor cores against the FP64 ZGEMM Gram, eigen-decomposition,
+    # projection, timed on the device
     clutter = None
     if not a.no_clutter and rank == 0:
         try:
-            from simu_rca_ab_b200.clutter import svd_clutter_filter
-            x = out[:, 0]
-            svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C")
-            torch.cuda.synchronize()
-            c0e, c1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            c0e.record()
-            xf, ev = svd_clutter_filter(x, None, (0.1,), "high", time_axis=0, order="C")
-            c1e.record()
-            torch.cuda.synchronize()
-            clutter = {"what": "SVDClutterFilter high-pass w=0.1 on the beamformed ensemble "
-                               f"({x.shape[1]} voxels x {x.shape[0]} frames): FP64 Gram (cuBLAS ZGEMM), "
-                               "FP64 eigh, FP32 projection (CGEMM)",
-                       "ms": c0e.elapsed_time(c1e),
-                       "energy_kept": float((xf.abs() ** 2).sum() / (x.abs() ** 2).sum())}
-            del xf
+            clutter = clutter_leg(out[:, 0], dev)
         except Exception as ex:
             clutter = {"error": f"{type(ex).__name__}: {ex}"}
 

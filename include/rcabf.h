@@ -488,6 +488,45 @@ int rcabf_take_launch_count(int64_t *count);
  * FP32 roofline.  Synchronises the stream. */
 int rcabf_measure_fp32_peak(double *tflops, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Casorati Gram matrix of the SVD clutter filter on the tensor cores.
+ *
+ * Replaces the IQf' * IQf product of SVDClutterFilter.m:23-25
+ * (MATLAB/lib/clutterFilter/SVDClutterFilter.m), which the reference forms in
+ * double precision before svd().  x: device complex64 [n_frame][ld], frame t's
+ * n_pix pixels at x[t * ld .. t * ld + n_pix) (the beamformer's ensemble
+ * layout, frame-major: the transpose of reshape(IQ, [], nT)).  G: device
+ * complex128 [n_frame][n_frame], row-major, G[i][j] = sum_p conj(x[i][p])
+ * x[j][p] = (C' * C)(i, j); Hermitian, written in full.
+ *
+ * Arithmetic: each value is cut into four signed 7-bit integer slices under a
+ * power-of-two scale per (frame part, chunk of chunk_voxels pixels), the
+ * slice products run on int8 tensor cores with exact int32 accumulation, and
+ * the levels and chunks combine in FP64; relative to an FP64 Gram the error is
+ * at most 2^-27 of each chunk's largest value per term (measured ~1e-10 of
+ * max|G|), and the result is deterministic.  Chunk rows whose largest
+ * magnitude is below 2^-100 count as zero.  chunk_voxels: 0 for the default
+ * (16384), else a multiple of 64 up to 65536.
+ * ------------------------------------------------------------------------- */
+typedef struct rcabf_gram_plan {
+    int32_t struct_size;      /* sizeof(rcabf_gram_plan) */
+    int32_t chunk_voxels;     /* pixels per scaling chunk */
+    int32_t n_chunks;
+    int32_t column_block;     /* columns of the 2 n_frame x 2 n_frame real Gram per tile (MMA N) */
+    int32_t n_tiles;          /* 128 x column_block tiles formed per chunk (upper triangle) */
+    int32_t launches;         /* kernel launches per call */
+    size_t workspace_bytes;   /* device workspace rcabf_casorati_gram needs */
+    double mma_int_ops;       /* 2 x int8 multiply-adds issued to the tensor cores per call */
+} rcabf_gram_plan;
+
+int rcabf_casorati_gram_plan(int64_t n_frame, int64_t n_pix, int32_t chunk_voxels, rcabf_gram_plan *out);
+
+/* Gram of x into G (see above); workspace: device, 256-byte aligned, at least
+ * rcabf_gram_plan.workspace_bytes.  Asynchronous on `stream`.  A bounded wait
+ * that gives up counts in rcabf_take_error_count. */
+int rcabf_casorati_gram(void *G, const void *x, int64_t n_frame, int64_t n_pix, int64_t ld, int32_t chunk_voxels,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,14 @@ class UlmBins(C.Structure):
     ]
 
 
+class GramPlan(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_int32), ("chunk_voxels", C.c_int32), ("n_chunks", C.c_int32),
+        ("column_block", C.c_int32), ("n_tiles", C.c_int32), ("launches", C.c_int32),
+        ("workspace_bytes", C.c_size_t), ("mma_int_ops", C.c_double),
+    ]
+
+
 # Every symbol include/rcabf.h declares, with its ctypes signature.
 _SIGS = {
     "rcabf_status_string": (C.c_char_p, [C.c_int]),
@@ -149,6 +157,9 @@ _SIGS = {
     "rcabf_take_error_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_take_launch_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "rcabf_measure_fp32_peak": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
+    "rcabf_casorati_gram_plan": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.POINTER(GramPlan)]),
+    "rcabf_casorati_gram": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32,
+                                      C.c_void_p, C.c_size_t, C.c_void_p]),
 }
 
 _lib = None

@@ -11,13 +11,18 @@ Doppler ensemble the beamformer produces:
 4. keep the components the filter type selects from round(w * nT) and
    project: C_f = C V V^H.
 
-Steps 2 and 4 are plain dense complex GEMMs (nT x nT x pixels): the Gram
-runs as a cuBLAS ZGEMM in FP64, as the reference forms it in double (the
-eigen-components the filter separates span 60 dB and more), the projection
-as a CGEMM in FP32 with TF32 off (its error is relative to the input
-magnitude, ~1e-7); step 3 runs in FP64 on the device (cuSOLVER through
-torch.linalg.eigh) on the nT x nT matrix.  For the C2 ensemble (1.47M voxels
-x 200 frames) each GEMM is 2.4e11 real multiply-adds x 2.
+Step 2 is the dense contraction (nT x nT x pixels; 2.4e11 real
+multiply-adds for the C2 ensemble of 1.47M voxels x 200 frames).  The
+reference forms it in double (the eigen-components the filter separates span
+60 dB and more); here it runs on the int8 tensor cores
+(``rcabf_casorati_gram``, casorati_gram.cu): every FP32 value is cut into
+four 7-bit integer slices under a power-of-two scale per (frame part, chunk
+of pixels), the slice products accumulate exactly in int32, and levels and
+chunks combine in FP64 -- about 1e-10 of max|G| from an FP64 Gram.
+``gram="fp64"`` forms it instead as a cuBLAS ZGEMM in FP64 (the comparator).
+Step 3 runs in FP64 on the device (cuSOLVER through torch.linalg.eigh) on
+the nT x nT matrix; step 4, the projection, is a CGEMM in FP32 with TF32 off
+(its error is relative to the input magnitude, ~1e-7).
 
 The beamformer's output [frame][pixel] is already the Casorati matrix's
 transpose in memory (pixel fastest, as MATLAB's reshape(IQ, [], nT)), so no
@@ -50,6 +55,43 @@ def keep_components(n: int, w, kind: str = "band") -> np.ndarray:
     return (idx >= ncut[0]) & (idx <= ncut[1])
 
 
+def gram_plan(n_frame: int, n_pix: int, chunk_voxels: int = 0) -> dict:
+    """Tile plan of the tensor-core Gram (rcabf_gram_plan) as a dict."""
+    import ctypes as C
+
+    from . import _lib as L
+    p = L.GramPlan()
+    p.struct_size = C.sizeof(L.GramPlan)
+    L.check(L.lib().rcabf_casorati_gram_plan(int(n_frame), int(n_pix), int(chunk_voxels), C.byref(p)),
+            "rcabf_casorati_gram_plan")
+    return {k: getattr(p, k) for k, _ in L.GramPlan._fields_ if k != "struct_size"}
+
+
+def casorati_gram(x: torch.Tensor, chunk_voxels: int = 0, workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """G = conj(x) x^T (complex128, nT x nT) of a [frame][pixel] complex64
+    CUDA tensor on the int8 tensor cores: the IQf' * IQf of
+    SVDClutterFilter.m:25 with IQf = x^T.  Rows may be strided (pixels
+    contiguous).  Raises if librcabf is missing (no other path)."""
+    from . import _lib as L
+    if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.complex64 and x.ndim == 2):
+        raise ValueError("x must be a 2-D complex64 CUDA tensor [frame][pixel]")
+    if x.stride(1) != 1:
+        x = x.contiguous()
+    n_t, n_pix = x.shape
+    plan = gram_plan(n_t, n_pix, chunk_voxels)
+    nbytes = int(plan["workspace_bytes"])
+    if workspace is None or workspace.numel() < nbytes + 256:
+        workspace = torch.empty(nbytes + 256, dtype=torch.uint8, device=x.device)
+    base = workspace.data_ptr()
+    ws = base + ((-base) % 256)
+    g = torch.empty((n_t, n_t), dtype=torch.complex128, device=x.device)
+    with torch.cuda.device(x.device):
+        st = torch.cuda.current_stream(x.device).cuda_stream
+        L.check(L.lib().rcabf_casorati_gram(g.data_ptr(), x.data_ptr(), n_t, n_pix, x.stride(0), int(chunk_voxels),
+                                            ws, nbytes, st), "rcabf_casorati_gram")
+    return g
+
+
 def _casorati_t(iq: torch.Tensor, time_axis: int) -> torch.Tensor:
     """[time][pixels] view (or copy) of an ensemble."""
     x = iq.movedim(time_axis, 0)
@@ -57,7 +99,7 @@ def _casorati_t(iq: torch.Tensor, time_axis: int) -> torch.Tensor:
 
 
 def svd_clutter_filter(IQ, Mask=None, w=(0.0, 1.0), type: str = "band", *, time_axis: int = -1,
-                       order: str = "F", keep: np.ndarray | None = None):
+                       order: str = "F", keep: np.ndarray | None = None, gram: str = "tensor_core"):
     """SVD clutter filter of an ensemble; returns (IQf, eig_val).
 
     IQ: complex tensor (CUDA) or array, time along ``time_axis``.  ``order``
@@ -66,8 +108,11 @@ def svd_clutter_filter(IQ, Mask=None, w=(0.0, 1.0), type: str = "band", *, time_
     itself does not depend on the pixel order).  Mask: per-pixel noise
     weights (same pixel shape), or None.  ``keep`` overrides (w, type) with
     an explicit boolean mask of components.  IQf has IQ's shape and stays
-    weighted by 1/sqrt(Mask), as in the reference.
+    weighted by 1/sqrt(Mask), as in the reference.  ``gram``: "tensor_core"
+    (the int8 slice Gram) or "fp64" (cuBLAS ZGEMM).
     """
+    if gram not in ("tensor_core", "fp64"):
+        raise ValueError("gram must be 'tensor_core' or 'fp64'")
     if not torch.cuda.is_available():
         raise RuntimeError("the clutter filter runs on a CUDA device; no CPU path exists")
     as_numpy = not isinstance(IQ, torch.Tensor)
@@ -97,12 +142,15 @@ def svd_clutter_filter(IQ, Mask=None, w=(0.0, 1.0), type: str = "band", *, time_
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     try:
-        # G[i][j] = sum_p conj(x_i) x_j in FP64 (the reference forms it in
-        # double: tissue clutter sits 40-60 dB above blood, so an FP32 Gram
-        # would blur the weak eigen-components the filter separates)
-        x64 = x.to(torch.complex128)
-        g = x64.conj() @ x64.T
-        del x64
+        # G[i][j] = sum_p conj(x_i) x_j at FP64 accuracy (the reference forms
+        # it in double: tissue clutter sits 40-60 dB above blood, so an FP32
+        # Gram would blur the weak eigen-components the filter separates)
+        if gram == "tensor_core":
+            g = casorati_gram(x)
+        else:
+            x64 = x.to(torch.complex128)
+            g = x64.conj() @ x64.T
+            del x64
         ev, vec = torch.linalg.eigh(g)                         # ascending
         ev, vec = ev.flip(0), vec.flip(1)                      # descending, as svd(G)
         k = keep if keep is not None else keep_components(n_t, w, type)

@@ -64,6 +64,15 @@ DeviceState *device_state(int dev, bool with_err = true)
     return s;
 }
 
+unsigned long long *current_error_counter()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    return device_state(dev)->err;
+}
+
+void count_launches(int64_t n) { g_launches += n; }
+
 static int pow2_ceil(int64_t x)
 {
     int p = 1;

@@ -79,6 +79,12 @@ cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, in
                             unsigned long long *err, int n_sm, cudaStream_t st);
 int tc_max_frames_per_block(int split);
 int tc_tmem_columns(int fb, int split);
+
+// The current device's bound-check / timeout counter (allocated on first use;
+// read and cleared by rcabf_take_error_count), and the library's count of
+// kernel launches (rcabf_take_launch_count).
+unsigned long long *current_error_counter();
+void count_launches(int64_t n);
 size_t tc_launch_smem(int fb);
 
 // Plain kernel: one frame.

@@ -206,3 +206,42 @@ def test_bf_iq_rca_pmig_matches_bf_rca_and_fp64(bf, cuda):
     rms, _ = H.error_db(iq.reshape(-1, F, order="F").T[:, pix], ref)
     print(f"BfIQRCA vs FP64: {rms:.1f} dB RMS")
     assert rms <= DB_TOL
+
+
+def test_per_transmit_output_past_2_31_elements(cuda):
+    """Per-transmit output (no compounding) of 140 frames of the Doppler
+    ensemble geometry: 140 x 11 x 1.47M = 2.27e9 output elements (18 GB),
+    past the 2^31 that limits the reference's int indexing and frame chunks
+    (bfVirtualSourceGeneric_RCA.m:587-594).  The last 4 frames, whose
+    outputs sit past element 2^31, equal the same 4 frames beamformed alone."""
+    import torch
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import beamformer as B
+    from simu_rca_ab_b200 import workloads as W
+    from simu_rca_ab_b200.params import normalize
+    w = W.get("c2", n_frame=140)
+    g0 = w.groups[0]
+    data = W.channel_data(w, seed=21, device="cuda").to(torch.complex32)
+    eng = B.default_engine()
+    geom = _quiet(eng.geometry, normalize(np.zeros(1, np.complex64), g0.Geometry, g0.Transmit, w.Param, w.Options))
+    n_tx, n_pix = geom.n_tx, geom.n_pix
+    assert 140 * n_tx * n_pix > 2 ** 31
+
+    def run(iq, n_frame):
+        out = torch.empty((n_frame, n_tx, n_pix), dtype=torch.complex64, device="cuda")
+        a = eng.make_args(geom, iq, iq_dtype=L.IQ_C32, n_sample=w.n_sample, n_frame=n_frame, out=out, mask=None,
+                          compound=False, storage=L.STORE_F16)
+        eng.run(geom, a)
+        torch.cuda.synchronize()
+        return out
+
+    big = run(data.contiguous(), 140)
+    tail = big[136:].cpu().numpy()
+    first = big[0, 0].abs().amax().item()
+    del big
+    torch.cuda.empty_cache()
+    alone = run(data[136:].contiguous(), 4).cpu().numpy()
+    rel = H.rel_rms(tail, alone)
+    print(f"per-transmit output of 140 frames (2.27e9 elements): last 4 frames vs alone rel {rel:.2e}")
+    assert first > 0 and np.isfinite(tail).all() and np.abs(tail).max() > 0
+    assert rel < 1e-6
