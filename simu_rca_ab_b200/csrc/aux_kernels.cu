@@ -25,7 +25,7 @@ template <> __device__ __forceinline__ __nv_bfloat162 from_f2<ST_BF16>(float2 v)
 
 constexpr int INGEST_NS = 64;
 constexpr int INGEST_FCHUNK = 64;    // frames of a block one CTA moves
-constexpr int INGEST_MAX_FB = 128;
+constexpr int INGEST_MAX_FB = 256;
 
 // grid.y = frame block x chunk of up to INGEST_FCHUNK of its frames
 template <int STORE, int IQ>

@@ -17,12 +17,24 @@
 // imaginary parts of W in two matrices one accumulator takes both:
 //     D = Re(W) . S + Im(W) . S'    (N = 2 FB columns, (re, im) per frame)
 // i.e. D[re] = Re(W) S_re - Im(W) S_im, D[im] = Re(W) S_im + Im(W) S_re.
+// The accumulator holds N = 2 FB FP32 columns, up to 416 (frame blocks up to
+// 208 frames; 232 with single FP16 weights): one MMA instruction covers at
+// most N = 256, so wider blocks issue two per weight matrix (columns
+// [0, 256) and [256, N), the second B operand starting at its fifth 64-element
+// panel).  Frame blocks are as wide as the tensor memory allows because the
+// weights are built once per (tile, step, frame block): the builders' work
+// per frame falls as the block grows, while the MMA work per frame stays.
 // Weights are formed in FP32 exactly as the SIMT kernels form them (degree-6
 // polynomials, FP32 phasors) and enter the MMA as FP16: SPLIT = true adds a
 // second FP16 term holding the remainder (hi + lo carries ~22 bits, the MMA
 // products are exact and summed in FP32), SPLIT = false keeps the single
 // FP16 rounding (~11 bits).  All weights are scaled by 2^8 (undone in the
 // epilogue) so that the remainder terms stay out of the FP16 subnormal range.
+//
+// Records.  A step's window is one or two 16-row chunks; each chunk is one
+// record (one K = 16 slice of the contraction), so every record has the same
+// shape: one weight slot of NMAT matrices of 8 tensor-memory columns, one
+// window stage of 16 rows of S and of S'.
 //
 // Roles (448 threads): three groups of four warps build the weight
 // matrices, one voxel per thread, straight into tensor memory (lane = voxel
@@ -31,24 +43,25 @@
 // group that
 // meets an item's end record writes that item's outputs; warp 12 computes
 // the windows of 32 steps at a time; each of its lanes with an active step
-// writes that step's record and loads its window with 3-D TMA (128-byte
-// swizzle) into its own stage of a ring of TC_NSB shared-memory stages, up
-// to TC_NSB records ahead of the MMAs, so the load latency stays off the
-// critical path; warp 13 issues the MMAs (A from one of TC_NSA tensor-memory
-// weight slots, B from shared memory) and commits them to the stage's
-// "empty" barrier, which also tells the builders the slot is free.  Steps whose window is empty for the whole
-// tile are skipped by every role alike: the producer passes each active
-// step's record (step, window start, 16-row chunks, item) through a ring of
-// TC_NSR record slots -- the builders start on a record as soon as it is
-// written, ahead of its window's load -- then an end-of-item record (with
-// the item's count of active steps), and after the last item one final
-// record per builder group.  Every wait
+// writes that step's chunk records and loads their rows with 3-D TMA
+// (128-byte swizzle) into their stages of a ring of TC_NSB shared-memory
+// stages, up to TC_NSB records ahead of the MMAs, so the load latency stays
+// off the critical path; warp 13 issues the MMAs (A from one of TC_NSA
+// tensor-memory weight slots, B from shared memory) and commits them to the
+// stage's "empty" barrier, which also tells the builders the slot is free.
+// Steps whose window is empty for the whole tile are skipped by every role
+// alike: the producer passes each active chunk's record (step, window
+// start, window chunks, chunk, item) through a ring of TC_NSR record slots
+// -- the builders start on a record as soon as it is written, ahead of its
+// rows' load -- then an end-of-item record (with the item's count of
+// records), and after the last item one final record per builder group.
+// Every wait
 // is bounded (mbar_wait): a wait that runs out sets an abort flag, counts an
 // error and every role leaves its loop.
 //
-// Tensor memory (512 columns, one CTA per SM): D at column 0 (N16 <= 256
-// columns), then TC_NSA slots of NMAT weight matrices of 16 columns (32 FP16
-// per row: K <= 32).
+// Tensor memory (512 columns, one CTA per SM): D at column 0 (N16 <= 416
+// columns), then TC_NSA slots of NMAT weight matrices of 8 columns (16 FP16
+// per row: K = 16).
 #pragma once
 
 #include <cuda.h>
@@ -64,29 +77,33 @@ namespace rcabf {
 constexpr int TC_GROUPS = 3;               // builder groups of 4 warps
 constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
 constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
-constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (K <= 32)
-constexpr int TC_NSA = TC_GROUPS;          // weight-matrix slots in tensor memory: group g uses slot g
+constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (windows <= 32 rows)
+constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory: record q uses slot q mod TC_NSA
 constexpr int TC_NSB = 6;                  // window stages in shared memory
 static_assert(TC_GROUPS <= TC_NSB, "the final records are written in one round");
 static_assert(TC_NSB > TC_NSA, "slot reuse is signalled through the window stages");
 constexpr int TC_NSR = 2 * TC_NSB;         // records in flight (a ring of its own, ahead of the window loads)
 static_assert(TC_NSR >= TC_NSB, "a record is written before its window is loaded");
-// A stage holds the window of S and of S', each TC_KCH chunks of 16 rows; a
-// chunk is tc_panels(fb)
-// 64-element panels of 16 rows x 128 bytes (2048 bytes each, 128-byte
-// swizzle), loaded by one 3-D TMA (x = element in the panel, y = row,
-// z = panel); the MMA's leading offset is the 2048-byte panel step.
+// A stage holds one 16-row chunk of S and the same rows of S'; a chunk is
+// tc_panels(fb) 64-element panels of 16 rows x 128 bytes (2048 bytes each,
+// 128-byte swizzle), loaded by one 3-D TMA (x = element in the panel,
+// y = row, z = panel); the MMA's leading offset is the 2048-byte panel step.
 constexpr int TC_PANEL_BYTES = 2048;
 constexpr float TC_SCALE = 256.0f;
+constexpr int TC_NMAX = 256;              // widest N of one MMA instruction (M = 128)
 constexpr RCABF_HD int tc_nmat(bool split) { return split ? 4 : 2; }
 constexpr RCABF_HD int tc_n16(int fb) { return (2 * fb + 15) / 16 * 16; }
 constexpr RCABF_HD int tc_panels(int fb) { return (2 * fb + 63) / 64; }
 // tensor-memory columns the kernel needs at frame block fb
-constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return tc_n16(fb) + TC_NSA * (split ? 4 : 2) * 16; }
-// largest frame block: the MMA's N = 2 FB is at most 256
-constexpr RCABF_HD int tc_max_fb(bool split) { return split ? 128 : 128; }
+constexpr RCABF_HD int tc_tmem_cols(int fb, bool split) { return tc_n16(fb) + TC_NSA * tc_nmat(split) * 8; }
+// largest frame block (a multiple of 8): the accumulator and the weight
+// slots share the 512 tensor-memory columns (208 frames with hi +
+// remainder weights, 232 with single FP16 weights)
+constexpr RCABF_HD int tc_max_fb(bool split) { return (512 - TC_NSA * tc_nmat(split) * 8) / 2 / 8 * 8; }
 // dynamic shared memory: TC_NSB stages of B panels + 1 KB for the 1024-byte alignment
-constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * 2 * TC_KCH * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+constexpr RCABF_HD size_t tc_smem_bytes(int fb) { return (size_t)TC_NSB * 2 * tc_panels(fb) * TC_PANEL_BYTES + 1024; }
+static_assert(tc_smem_bytes(232) <= 227 * 1024 - 2048, "window stages fit the shared memory at the widest block");
+static_assert(tc_tmem_cols(208, true) <= 512 && tc_tmem_cols(232, false) <= 512, "tensor-memory budget");
 
 // All lanes wait on the barrier; the warp proceeds (converged) only if every
 // lane saw the phase complete.
@@ -96,19 +113,21 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volati
     return __all_sync(0xffffffffu, ok);
 }
 
-// One record of the stage ring.  kind: TC_STEP (an active step: s, window
-// start lo, nk 16-row chunks), TC_END (end of item `it`, n active steps),
-// TC_FINAL (no more items).  it counts the CTA's items.
+// One record of the stage ring.  kind: TC_STEP (chunk ch of an active
+// step's window: step s, window start lo, nk 16-row chunks in the window),
+// TC_END (end of item `it`, n records), TC_FINAL (no more items).  it counts
+// the CTA's items.
 enum TcKind : int32_t { TC_STEP = 0, TC_END = 1, TC_FINAL = 2 };
 struct TcInfo {
-    int32_t kind, s, lo, nk, it, n, tx, rx;
+    int32_t kind, s, lo, nk, ch, it, n, tx, rx;
 };
 // a record written by another thread (published through an mbarrier)
 __device__ __forceinline__ TcInfo read_info(const TcInfo *p)
 {
     const volatile TcInfo *v = p;
     TcInfo r;
-    r.kind = v->kind; r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.it = v->it; r.n = v->n; r.tx = v->tx; r.rx = v->rx;
+    r.kind = v->kind; r.s = v->s; r.lo = v->lo; r.nk = v->nk; r.ch = v->ch; r.it = v->it; r.n = v->n;
+    r.tx = v->tx; r.rx = v->rx;
     return r;
 }
 
@@ -121,6 +140,17 @@ struct TcParams {
     int64_t n_items;            // n_fb * tiles
     unsigned long long *err_count;
 };
+
+// Tile coordinates of a tile index, depth slowest: the CTAs working at one
+// time hold tiles of one or two depths, whose windows of a step cover a few
+// dozen of the slab's rows, so the rows they read stay in L2 while the CTAs
+// drift apart across the steps.
+__device__ __forceinline__ void tc_tile_coords(const FusedJob &J, int64_t tile, int &tu, int &tv, int &tz)
+{
+    tu = (int)(tile % J.tiles_u);
+    tv = (int)((tile / J.tiles_u) % J.tiles_v);
+    tz = (int)(tile / ((int64_t)J.tiles_u * J.tiles_v));
+}
 
 // One step's window for the tile (producer): rows [lo, lo + 16 nk) of the
 // step's slab cover every tap of every voxel of the tile.
@@ -189,14 +219,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const FusedJob &J = prm.job;
     const DevGeom &g = J.g;
     const int FB = prm.fb;
-    const int NH = 2 * FB;                 // halfs per slab row = MMA N
-    const int N16 = tc_n16(FB);
+    const int NH = 2 * FB;                 // halfs per slab row
+    const int N16 = tc_n16(FB);            // accumulator columns
     const int NP = tc_panels(FB);
-    const int chunk_bytes = NP * TC_PANEL_BYTES;
-    const int half_bytes = TC_KCH * chunk_bytes;   // the S window; the S' window follows
-    const int stage_bytes = 2 * half_bytes;
+    const int chunk_bytes = NP * TC_PANEL_BYTES;   // 16 rows of S; the same rows of S' follow
+    const int stage_bytes = 2 * chunk_bytes;
     const int a_col0 = N16;                // first weight-matrix column
-    const uint32_t idesc = idesc_f16_kmaj_a_mnmaj_b(128, N16);
+    // one MMA per weight matrix covers columns [0, n_a); a second one
+    // [TC_NMAX, N16) when the block is wider (its B operand starts at panel
+    // TC_NMAX / 64)
+    const int n_a = N16 < TC_NMAX ? N16 : TC_NMAX;
+    const int n_b = N16 - n_a;
+    const uint32_t idesc_a = idesc_f16_kmaj_a_mnmaj_b(128, n_a);
+    const uint32_t idesc_b = idesc_f16_kmaj_a_mnmaj_b(128, n_b > 0 ? n_b : 16);
 
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], rec_full[TC_NSR], rec_empty[TC_NSR];
@@ -252,9 +287,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     if (warp == TC_PRODUCER_WARP) {
         // ---------------- producer: windows and TMA loads ----------------
         // The warp computes the windows of 32 steps at a time; each lane with
-        // an active step then writes that step's record itself (its place in
-        // the ring is the step's rank among the active ones), TC_NSB lanes at
-        // a time, each lane waiting on its own stage.
+        // an active step then writes that step's chunk records itself (their
+        // places in the ring follow the records of the lanes below), TC_NSB
+        // records at a time, each lane waiting on its own stages.
         if (lane == 0) tma_prefetch_desc(&prm.tmap);
         uint32_t q = 0;          // next record (warp-uniform)
         bool stop = false;       // warp-uniform after each batch
@@ -271,13 +306,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             if (!mbar_wait(&empty_b[st], ((qr / TC_NSB) & 1u) ^ 1u, abort)) return false;
             if (rec.kind == TC_STEP) {
                 last_rec[st] = (int)qr;
-                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * rec.nk * chunk_bytes));
+                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * chunk_bytes));
                 uint8_t *dst = Bs + st * stage_bytes;
-                for (int j = 0; j < rec.nk; ++j) {
-                    tma_load_3d(dst + j * chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(row0 + 16 * j), 0);
-                    tma_load_3d(dst + half_bytes + j * chunk_bytes, &prm.tmap, &full_b[st], 0,
-                                (int32_t)(prm.s2_row0 + row0 + 16 * j), 0);
-                }
+                tma_load_3d(dst, &prm.tmap, &full_b[st], 0, (int32_t)row0, 0);
+                tma_load_3d(dst + chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(prm.s2_row0 + row0), 0);
             } else {
                 last_rec[st] = -1;   // no copy in flight
                 mbar_arrive(&full_b[st]);
@@ -288,9 +320,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x, ++it) {
             const int fb = (int)(item / n_tiles);
             const int64_t tile = item % n_tiles;
-            const int tz = (int)(tile % J.tiles_z);
-            const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
-            const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+            int tu, tv, tz;
+            tc_tile_coords(J, tile, tu, tv, tz);
             int n_active = 0;
             for (int s0 = 0; s0 < n_steps && !stop; s0 += 32) {
                 const int s = s0 + lane;
@@ -302,34 +333,45 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     act = tc_window<KIND>(J, s, tx, rx, tu, tv, tz, lo, nk, ovf);
                     if (ovf) atomicAdd(prm.err_count, 1ull);   // never expected: the planner bounds the window
                 }
-                const unsigned mask = __ballot_sync(0xffffffffu, act);
-                const int n_act = __popc(mask);
-                const int rank = __popc(mask & ((1u << lane) - 1u));
+                // the step's chunk records follow the records of the lanes
+                // below it (exclusive prefix sum of the chunk counts)
+                const int cnt = act ? nk : 0;
+                int incl = cnt;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                const int base = incl - cnt;
+                const int n_rec = __shfl_sync(0xffffffffu, incl, 31);
                 // in rounds of at most TC_NSB records: a stage's barrier
                 // tells apart only the phase of its previous use, so no lane
                 // may wait on a stage more than one use ahead of the records
                 // already written
-                for (int r0 = 0; r0 < n_act && !stop; r0 += TC_NSB) {
+                for (int r0 = 0; r0 < n_rec && !stop; r0 += TC_NSB) {
                     bool ok = true;
-                    if (act && rank >= r0 && rank < r0 + TC_NSB) {
-                        const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo;
-                        ok = emit(q + (uint32_t)rank, TcInfo{TC_STEP, s, lo, nk, it, 0, tx, rx}, row0);
+                    for (int j = 0; j < cnt && ok; ++j) {
+                        const int r = base + j;
+                        if (r >= r0 && r < r0 + TC_NSB) {
+                            const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo + 16 * j;
+                            ok = emit(q + (uint32_t)r, TcInfo{TC_STEP, s, lo, nk, j, it, 0, tx, rx}, row0);
+                        }
                     }
                     stop = __any_sync(0xffffffffu, !ok);
                 }
-                q += (uint32_t)n_act;
-                n_active += n_act;
+                q += (uint32_t)n_rec;
+                n_active += n_rec;
             }
             if (!stop) {   // end of item
                 bool ok = true;
-                if (lane == 0) ok = emit(q, TcInfo{TC_END, 0, 0, 0, it, n_active, 0, 0}, 0);
+                if (lane == 0) ok = emit(q, TcInfo{TC_END, 0, 0, 0, 0, it, n_active, 0, 0}, 0);
                 stop = __any_sync(0xffffffffu, !ok);
                 ++q;
             }
         }
         if (!stop) {   // one final record per builder group (TC_GROUPS <= TC_NSB)
             bool ok = true;
-            if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, it, 0, 0, 0}, 0);
+            if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, 0, it, 0, 0, 0}, 0);
             stop = __any_sync(0xffffffffu, !ok);
         }
         if (lane == 0 && stop) {
@@ -363,7 +405,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 }
                 if (inf.kind == TC_END) {
                     umma_commit(&acc_full);
-                    mbar_arrive(&empty_b[bst]);
+                    // released once the MMAs issued so far have completed,
+                    // like the stages of step records
+                    umma_commit(&empty_b[bst]);
                     mbar_arrive(&rec_empty[rs]);
                     first = true;
                     dacc = false;
@@ -371,17 +415,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 }
                 tmem_fence_after_sync();
                 const uint32_t bbase = smem_u32(Bs + bst * stage_bytes);
-                const uint32_t acol = (uint32_t)(a_col0 + ast * NMAT * 16);
-                for (int j = 0; j < inf.nk; ++j) {
-                    const uint64_t bs = sdesc_mn_sw128(bbase + j * chunk_bytes, TC_PANEL_BYTES, 1024);
-                    const uint64_t bs2 = sdesc_mn_sw128(bbase + half_bytes + j * chunk_bytes, TC_PANEL_BYTES, 1024);
+                const uint32_t acol = (uint32_t)(a_col0 + ast * NMAT * 8);
+                const uint32_t acc0 = dacc ? 1u : 0u;   // the item's first record starts the sums
 #pragma unroll
-                    for (int mat = 0; mat < NMAT; ++mat) {
-                        // Re(W) against S, Im(W) against S' = (-im, re)
-                        umma_f16_ts(tb, tb + acol + mat * 16 + 8 * j, mat < NMAT / 2 ? bs : bs2, idesc, dacc ? 1u : 0u);
-                        dacc = true;
-                    }
+                for (int mat = 0; mat < NMAT; ++mat) {
+                    // Re(W) against S, Im(W) against S' = (-im, re)
+                    const uint32_t b0 = bbase + (mat < NMAT / 2 ? 0u : (uint32_t)chunk_bytes);
+                    const uint32_t acc = mat == 0 ? acc0 : 1u;
+                    umma_f16_ts(tb, tb + acol + mat * 8, sdesc_mn_sw128(b0, TC_PANEL_BYTES, 1024), idesc_a, acc);
+                    if (n_b > 0)
+                        umma_f16_ts(tb + (uint32_t)TC_NMAX, tb + acol + mat * 8,
+                                    sdesc_mn_sw128(b0 + (TC_NMAX / 64) * TC_PANEL_BYTES, TC_PANEL_BYTES, 1024),
+                                    idesc_b, acc);
                 }
+                dacc = true;
                 umma_commit(&empty_b[bst]);   // releases the stage and, for the builders, the weight slot
                 mbar_arrive(&rec_empty[rs]);
                 issued = true;
@@ -414,9 +461,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 const int64_t item = blockIdx.x + (int64_t)inf.it * gridDim.x;
                 fb = (int)(item / n_tiles);
                 const int64_t tile = item % n_tiles;
-                const int tz = (int)(tile % J.tiles_z);
-                const int tu = (int)((tile / J.tiles_z) % J.tiles_u);
-                const int tv = (int)(tile / ((int64_t)J.tiles_z * J.tiles_u));
+                int tu, tv, tz;
+                tc_tile_coords(J, tile, tu, tv, tz);
                 iz = tz; iu = (int64_t)tu * J.tu + lu; iv = (int64_t)tv * J.tv + lv;
                 valid = iz < g.n_z && iu < g.n_u && iv < g.n_v;
                 rxkey = valid ? iu * g.n_z + iz : 0;
@@ -425,13 +471,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 pre_s = -1;
             }
             const int ast = (int)(q % TC_NSA);
-            // the slot's previous use, record q - TC_NSA (built by this group),
-            // has been consumed: its MMAs completed, which the MMA warp
-            // signals on the window stage that record used.  That stage's
-            // barrier is at most one use behind or ahead of the wait (this
-            // group built record q - 2 TC_NSA only after record q - 3 TC_NSA
-            // was consumed, and record q + TC_NSB - TC_NSA is built after
-            // this one), so its parity identifies the use.
+            // the slot's previous use, record q - TC_NSA, has been consumed:
+            // its MMAs completed, which the MMA warp signals (tcgen05.commit,
+            // in record order) on the window stage that record used.  That
+            // stage's barrier has completed the use before it, record
+            // q - TC_NSA - TC_NSB (this group's previous record q - TC_GROUPS
+            // waited for the later record q - TC_GROUPS - TC_NSA, as
+            // TC_GROUPS <= TC_NSB), and not the use after it, record
+            // q + TC_NSB - TC_NSA (its MMAs follow this record's), so the
+            // parity identifies the use.
             auto wait_slot = [&]() -> bool {
                 if (q < (uint32_t)TC_NSA) return true;
                 const uint32_t qp = q - TC_NSA;
@@ -480,13 +528,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             float4 e;
             if (pre_s == inf.s) e = pre_e;
             else e = valid ? __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]) : make_float4(0.f, 0.f, 0.f, 0.f);
-            // this group's next record is most often two steps on: its
-            // receive entry is loaded while this one is built
-            if (valid && rx + TC_GROUPS < g.n_ele) {
-                pre_s = inf.s + TC_GROUPS;
-                pre_e = __ldg(&g.rx_tab[(int64_t)(rx + TC_GROUPS) * n_rxkey + rxkey]);
-            } else {
-                pre_s = -1;
+            // the receive entry of this group's next record is loaded while
+            // this one is built: that record's step when the producer has
+            // written it already (a test, no wait), else a guess three
+            // steps on
+            {
+                const uint32_t qn = q + TC_GROUPS;
+                const int rn = (int)(qn % TC_NSR);
+                int ns = inf.s + TC_GROUPS, nrx = rx + TC_GROUPS;
+                if (mbar_test_wait(&rec_full[rn], (qn / TC_NSR) & 1u)) {
+                    const volatile TcInfo *v = &info[rn];
+                    if (v->kind == TC_STEP) { ns = v->s; nrx = v->rx; }
+                }
+                if (valid && nrx < g.n_ele) {
+                    pre_s = ns;
+                    pre_e = __ldg(&g.rx_tab[(int64_t)nrx * n_rxkey + rxkey]);
+                } else {
+                    pre_s = -1;
+                }
             }
             const float ab = ab_value(g, tx, rx);
             const float2 abp = ab_phasor(g, tx, rx);
@@ -505,17 +564,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
             const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
             const float py = ok ? TC_SCALE * fmaf(qx, abp.y, qy * abp.x) : 0.0f;
-            const uint32_t acol = lane_base + (uint32_t)(a_col0 + ast * NMAT * 16);
+            const uint32_t acol = lane_base + (uint32_t)(a_col0 + ast * NMAT * 8);
             // the packed weight rows are formed in registers first; the wait
             // for the slot comes only before the stores, so that a group's
             // arithmetic overlaps the MMAs still reading the slot
-            auto build = [&](auto nkc) -> bool {
-                constexpr int NKC = decltype(nkc)::value;
-                float v[16 * NKC];
-                tc_place<TAPS, 16 * NKC>(w, o, v);
-                uint32_t words[NMAT][8 * NKC];
+            auto build = [&](auto wide) -> bool {
+                constexpr bool WIDE = decltype(wide)::value;
+                // the voxel's taps in this record's 16 rows: at o in a
+                // one-chunk window; in a two-chunk window at o - 16 ch,
+                // clipped to the chunk (placed at o + 16 - 16 ch over 32
+                // positions, of which the upper 16 are kept; a start past
+                // the end leaves the chunk empty)
+                float v[16];
+                if constexpr (WIDE) {
+                    const int e = o + 16 - 16 * inf.ch;
+                    float v32[32];
+                    tc_place<TAPS, 32>(w, e < 32 ? e : 0, v32);
 #pragma unroll
-                for (int c = 0; c < 8 * NKC; ++c) {
+                    for (int p = 0; p < 16; ++p) v[p] = v32[16 + p];
+                } else {
+                    tc_place<TAPS, 16>(w, o, v);
+                }
+                uint32_t words[NMAT][8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
                     const float ar = v[2 * c] * px, br = v[2 * c + 1] * px;
                     const float ai = v[2 * c] * py, bi = v[2 * c + 1] * py;
                     if constexpr (SPLIT) {
@@ -531,20 +603,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 if (!wait_slot()) return false;
                 tmem_fence_after_sync();
 #pragma unroll
-                for (int mat = 0; mat < NMAT; ++mat)
-#pragma unroll
-                    for (int j = 0; j < NKC; ++j) {
-                        uint32_t r8[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) r8[c] = words[mat][8 * j + c];
-                        tmem_st8(acol + (uint32_t)(mat * 16 + 8 * j), r8);
-                    }
+                for (int mat = 0; mat < NMAT; ++mat) tmem_st8(acol + (uint32_t)(mat * 8), words[mat]);
                 tmem_wait_st();
                 tmem_fence_before_sync();
                 return true;
             };
-            const bool built = inf.nk == 1 ? build(std::integral_constant<int, 1>{})
-                                           : build(std::integral_constant<int, 2>{});
+            const bool built = inf.nk == 1 ? build(std::false_type{}) : build(std::true_type{});
             if (!built) break;
             mbar_arrive(&full_a[ast]);
         }

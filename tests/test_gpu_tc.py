@@ -95,11 +95,14 @@ def test_tensor_core_kernel_vs_fp64_and_simt_on_the_ensemble_geometry(c2_40, kna
     assert np.isfinite(o).all()
 
 
-@pytest.mark.parametrize("kname,n_frame", [("tc", 100), ("tc16", 100), ("tc", 33), ("tc", 300)])
+@pytest.mark.parametrize("kname,n_frame", [("tc", 100), ("tc16", 100), ("tc", 33), ("tc", 300), ("tc", 200),
+                                           ("tc16", 232)])
 def test_frame_blocks_and_padding(cuda, kname, n_frame):
-    """One block of 104 frames for 100 frames (either weight precision) and a
-    block padded from 33 to 40 frames give every frame the SIMT kernel's
-    value."""
+    """One block of 104 frames for 100 frames (either weight precision), a
+    block padded from 33 to 40 frames, two blocks of 152 frames for 300, and
+    the widest blocks (200 frames with hi + remainder weights, 232 with single
+    FP16 weights: accumulators wider than one MMA's 256 columns) give every
+    frame the SIMT kernel's value."""
     from simu_rca_ab_b200 import _lib as L
     from simu_rca_ab_b200 import workloads as W
     w = W.get("c2", n_frame=n_frame)
@@ -108,6 +111,7 @@ def test_frame_blocks_and_padding(cuda, kname, n_frame):
     out, plan = _run(w, eng, geom, iq, kern)
     ref, _ = _run(w, eng, geom, iq, L.KERNEL_FUSED_TMEM)
     print(kname, n_frame, plan)
+    assert plan["frames_per_block"] == {100: 104, 33: 40, 300: 152, 200: 200, 232: 232}[n_frame]
     assert _errcount() == 0
     rel = H.rel_rms(out.cpu().numpy(), ref.cpu().numpy())
     assert rel < (2e-4 if kname == "tc" else 1e-3), rel
