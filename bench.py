@@ -744,35 +744,57 @@ def main():
     # the beamforming of its neighbours)
     e2e = None
     if not a.no_e2e:
-        host_in = [t.cpu().pin_memory() for t in iq_dev]
-        host_out = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
-        out_bytes = host_out.numel() * host_out.element_size()
+        # a stream of ensembles through the same call, as an acquisition loop
+        # issues them: two slots (pinned host buffers, device workspace,
+        # stream) alternate, so that one ensemble's copy out runs under the
+        # next one's copy in and beamforming; inside a call the frames also
+        # go through in chunks whose copies overlap their neighbours'
+        # beamforming.  The latency of one call alone is reported beside it.
+        streams = [stream, torch.cuda.Stream(dev)]
+        slots = []
+        for si in range(2):
+            h_in = [t.cpu().pin_memory() for t in iq_dev]
+            h_out = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+            h_mask = torch.empty_like(mask)
+            h_args = [eng.make_args(g, h_in[gi], iq_dtype=iq_code, n_sample=w.n_sample, n_frame=F, out=h_out,
+                                    mask=h_mask, compound=True, storage=st_code, kernel=kern, accumulate=gi > 0,
+                                    frames_per_block=a.frames_per_block, host=True)
+                      for gi, g in enumerate(geoms)]
+            slots.append((h_in, h_out, h_args))
+        out_bytes = out.numel() * out.element_size()
         # later groups add into the output: their chunks are read in as well
-        h2d = sum(t.numel() * t.element_size() for t in host_in) + out_bytes * (len(geoms) - 1)
+        h2d = sum(t.numel() * t.element_size() for t in slots[0][0]) + out_bytes * (len(geoms) - 1)
         d2h = out_bytes * len(geoms)
-        host_args = [eng.make_args(g, host_in[gi], iq_dtype=iq_code, n_sample=w.n_sample, n_frame=F, out=host_out,
-                                   mask=mask, compound=True, storage=st_code, kernel=kern, accumulate=gi > 0,
-                                   frames_per_block=a.frames_per_block, host=True)
-                     for gi, g in enumerate(geoms)]
 
-        def e2e_step():
-            for g, ar in zip(geoms, host_args):
-                eng.run_host(g, ar, 0, stream)
+        def e2e_call(k):
+            for g, ar in zip(geoms, slots[k % 2][2]):
+                eng.run_host(g, ar, 0, streams[k % 2])
 
-        for _ in range(2):
-            e2e_step()
+        for k in range(4):
+            e2e_call(k)
         torch.cuda.synchronize()
         barrier()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        e2e_call(0)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        lat_ms = l0.elapsed_time(l1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(a.steps):
-            e2e_step()
+        streams[1].wait_event(e0)
+        for k in range(a.steps):
+            e2e_call(k)
+        stream.wait_stream(streams[1])
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
         e2e_ms = max_over_ranks(e2e_ms, dev)
+        same = bool(torch.equal(slots[0][1], slots[1][1]))
         e2e = {"value": units * world * a.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / a.steps}
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / a.steps,
+               "call": "rcabf_beamform_host (host buffers in and out), two ensembles in flight on two streams",
+               "latency_one_call_ms": lat_ms, "slots_identical": same}
 
     # the plain one-launch-per-frame kernel on FP32 storage, complex64 input
     # (the comparator of the fused path), timed on a sample of the frames

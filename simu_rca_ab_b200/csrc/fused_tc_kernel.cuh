@@ -36,19 +36,22 @@
 // shape: one weight slot of NMAT matrices of 8 tensor-memory columns, one
 // window stage of 16 rows of S and of S'.
 //
-// Roles (448 threads): three groups of four warps build the weight
+// Roles (480 threads): three groups of four warps build the weight
 // matrices, one voxel per thread, straight into tensor memory (lane = voxel
 // row; tcgen05.st), taking records in turn (group g the records q with
 // q mod 3 = g, so that the groups' dependent setup chains overlap), and the
 // group that
-// meets an item's end record writes that item's outputs; warp 12 computes
-// the windows of 32 steps at a time; each of its lanes with an active step
-// writes that step's chunk records and loads their rows with 3-D TMA
-// (128-byte swizzle) into their stages of a ring of TC_NSB shared-memory
-// stages, up to TC_NSB records ahead of the MMAs, so the load latency stays
-// off the critical path; warp 13 issues the MMAs (A from one of TC_NSA
-// tensor-memory weight slots, B from shared memory) and commits them to the
-// stage's "empty" barrier, which also tells the builders the slot is free.
+// meets an item's end record writes that item's outputs; warp 12, the
+// producer, computes the windows of 32 steps at a time and each of its lanes
+// with an active step writes that step's chunk records into a ring of TC_NSR
+// record slots, at least TC_NPUB records ahead of the MMAs; warp 14, the
+// loader, follows the ring one record at a time and loads each record's rows
+// with 3-D TMA (128-byte swizzle) into its stage of a ring of TC_NSB
+// shared-memory stages as soon as that stage is free, so that the loads run
+// up to TC_NSB records ahead of the MMAs with no gap between rounds; warp 13
+// issues the MMAs (A from one of TC_NSA tensor-memory weight slots, B from
+// shared memory) and commits them to the stage's "empty" barrier, which also
+// tells the builders the slot is free.
 // Steps whose window is empty for the whole tile are skipped by every role
 // alike: the producer passes each active chunk's record (step, window
 // start, window chunks, chunk, item) through a ring of TC_NSR record slots
@@ -75,14 +78,15 @@
 namespace rcabf {
 
 constexpr int TC_GROUPS = 3;               // builder groups of 4 warps
-constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 2);
-constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1;
+constexpr int TC_THREADS = 32 * (4 * TC_GROUPS + 3);
+constexpr int TC_PRODUCER_WARP = 4 * TC_GROUPS, TC_MMA_WARP = 4 * TC_GROUPS + 1, TC_LOADER_WARP = 4 * TC_GROUPS + 2;
 constexpr int TC_KCH = TC_MAX_ROWS / 16;   // 16-row chunks per step window at most (windows <= 32 rows)
 constexpr int TC_NSA = 3;                  // weight-matrix slots in tensor memory: record q uses slot q mod TC_NSA
 constexpr int TC_NSB = 6;                  // window stages in shared memory
-static_assert(TC_GROUPS <= TC_NSB, "the final records are written in one round");
 static_assert(TC_NSB > TC_NSA, "slot reuse is signalled through the window stages");
 constexpr int TC_NSR = 2 * TC_NSB;         // records in flight (a ring of its own, ahead of the window loads)
+constexpr int TC_NPUB = TC_NSR / 2;        // records the producer writes per round
+static_assert(TC_GROUPS <= TC_NPUB, "the final records are written in one round");
 static_assert(TC_NSR >= TC_NSB, "a record is written before its window is loaded");
 // A stage holds one 16-row chunk of S and the same rows of S'; a chunk is
 // tc_panels(fb) 64-element panels of 16 rows x 128 bytes (2048 bytes each,
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], rec_full[TC_NSR], rec_empty[TC_NSR];
     __shared__ uint64_t acc_full, acc_empty, fin;
     __shared__ TcInfo info[TC_NSR];
-    __shared__ volatile int last_rec[TC_NSB];   // producer: latest record loaded into each stage, -1 none
+    __shared__ volatile int last_rec[TC_NSB];   // loader: latest record loaded into each stage, -1 none
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
     uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -285,40 +289,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     const int n_steps = g.n_tx * g.n_ele;
 
     if (warp == TC_PRODUCER_WARP) {
-        // ---------------- producer: windows and TMA loads ----------------
+        // ---------------- producer: windows and records ----------------
         // The warp computes the windows of 32 steps at a time; each lane with
         // an active step then writes that step's chunk records itself (their
-        // places in the ring follow the records of the lanes below), TC_NSB
-        // records at a time, each lane waiting on its own stages.
-        if (lane == 0) tma_prefetch_desc(&prm.tmap);
+        // places in the ring follow the records of the lanes below), TC_NPUB
+        // records at a time.  A record goes into its slot once the MMA warp
+        // is done with the record TC_NSR earlier; the builders and the loader
+        // pick it up from there.
         uint32_t q = 0;          // next record (warp-uniform)
         bool stop = false;       // warp-uniform after each batch
-        // a record first goes into its record slot (free once the MMA warp
-        // is done with the record TC_NSR earlier), where the builders pick it
-        // up; its window is then loaded into its stage (free once the MMAs of
-        // the record TC_NSB earlier completed), which the MMA warp waits for
-        auto emit = [&](uint32_t qr, const TcInfo rec, int64_t row0) -> bool {
+        auto emit = [&](uint32_t qr, const TcInfo rec) -> bool {
             const int rs = (int)(qr % TC_NSR);
             if (!mbar_wait(&rec_empty[rs], ((qr / TC_NSR) & 1u) ^ 1u, abort)) return false;
             info[rs] = rec;
             mbar_arrive(&rec_full[rs]);
-            const int st = (int)(qr % TC_NSB);
-            if (!mbar_wait(&empty_b[st], ((qr / TC_NSB) & 1u) ^ 1u, abort)) return false;
-            if (rec.kind == TC_STEP) {
-                last_rec[st] = (int)qr;
-                mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * chunk_bytes));
-                uint8_t *dst = Bs + st * stage_bytes;
-                tma_load_3d(dst, &prm.tmap, &full_b[st], 0, (int32_t)row0, 0);
-                tma_load_3d(dst + chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(prm.s2_row0 + row0), 0);
-            } else {
-                last_rec[st] = -1;   // no copy in flight
-                mbar_arrive(&full_b[st]);
-            }
             return true;
         };
         int it = 0;
         for (int64_t item = blockIdx.x; item < prm.n_items && !stop; item += gridDim.x, ++it) {
-            const int fb = (int)(item / n_tiles);
             const int64_t tile = item % n_tiles;
             int tu, tv, tz;
             tc_tile_coords(J, tile, tu, tv, tz);
@@ -344,18 +332,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 }
                 const int base = incl - cnt;
                 const int n_rec = __shfl_sync(0xffffffffu, incl, 31);
-                // in rounds of at most TC_NSB records: a stage's barrier
+                // in rounds of at most TC_NPUB records: a slot's barrier
                 // tells apart only the phase of its previous use, so no lane
-                // may wait on a stage more than one use ahead of the records
+                // may wait on a slot more than one use ahead of the records
                 // already written
-                for (int r0 = 0; r0 < n_rec && !stop; r0 += TC_NSB) {
+                for (int r0 = 0; r0 < n_rec && !stop; r0 += TC_NPUB) {
                     bool ok = true;
                     for (int j = 0; j < cnt && ok; ++j) {
                         const int r = base + j;
-                        if (r >= r0 && r < r0 + TC_NSB) {
-                            const int64_t row0 = ((int64_t)s * J.n_fb + fb) * prm.rows_per_slab + lo + 16 * j;
-                            ok = emit(q + (uint32_t)r, TcInfo{TC_STEP, s, lo, nk, j, it, 0, tx, rx}, row0);
-                        }
+                        if (r >= r0 && r < r0 + TC_NPUB)
+                            ok = emit(q + (uint32_t)r, TcInfo{TC_STEP, s, lo, nk, j, it, 0, tx, rx});
                     }
                     stop = __any_sync(0xffffffffu, !ok);
                 }
@@ -364,23 +350,52 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
             }
             if (!stop) {   // end of item
                 bool ok = true;
-                if (lane == 0) ok = emit(q, TcInfo{TC_END, 0, 0, 0, 0, it, n_active, 0, 0}, 0);
+                if (lane == 0) ok = emit(q, TcInfo{TC_END, 0, 0, 0, 0, it, n_active, 0, 0});
                 stop = __any_sync(0xffffffffu, !ok);
                 ++q;
             }
         }
-        if (!stop) {   // one final record per builder group (TC_GROUPS <= TC_NSB)
+        if (!stop) {   // one final record per builder group (TC_GROUPS <= TC_NPUB)
             bool ok = true;
-            if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, 0, it, 0, 0, 0}, 0);
+            if (lane < TC_GROUPS) ok = emit(q + (uint32_t)lane, TcInfo{TC_FINAL, 0, 0, 0, 0, it, 0, 0, 0});
             stop = __any_sync(0xffffffffu, !ok);
         }
-        if (lane == 0 && stop) {
-            // let the copies in flight land before the CTA's shared memory goes
-            for (int st = 0; st < TC_NSB; ++st)
-                if (last_rec[st] >= 0) {
-                    volatile int dummy = 0;
-                    mbar_wait(&full_b[st], ((uint32_t)last_rec[st] / TC_NSB) & 1u, &dummy, 100000000ull);
+    } else if (warp == TC_LOADER_WARP) {
+        // ---------------- loader: the records' rows, one record at a time ----------------
+        // Record q's rows go into stage q mod TC_NSB once the MMAs of record
+        // q - TC_NSB have completed; end records pass their stage on with no
+        // copy.  The waits are in record order, so each stage's barrier is at
+        // most one use behind the wait and its parity identifies the use.
+        if (lane == 0) {
+            tma_prefetch_desc(&prm.tmap);
+            for (uint32_t q = 0;; ++q) {
+                const int rs = (int)(q % TC_NSR), st = (int)(q % TC_NSB);
+                if (!mbar_wait(&rec_full[rs], (q / TC_NSR) & 1u, abort)) break;
+                const TcInfo inf = read_info(&info[rs]);
+                if (inf.kind == TC_FINAL) break;
+                if (!mbar_wait(&empty_b[st], ((q / TC_NSB) & 1u) ^ 1u, abort)) break;
+                if (inf.kind == TC_STEP) {
+                    const int64_t item = blockIdx.x + (int64_t)inf.it * gridDim.x;
+                    const int64_t fb = item / n_tiles;
+                    const int64_t row0 = ((int64_t)inf.s * J.n_fb + fb) * prm.rows_per_slab + inf.lo + 16 * inf.ch;
+                    last_rec[st] = (int)q;
+                    mbar_arrive_expect_tx(&full_b[st], (uint32_t)(2 * chunk_bytes));
+                    uint8_t *dst = Bs + st * stage_bytes;
+                    tma_load_3d(dst, &prm.tmap, &full_b[st], 0, (int32_t)row0, 0);
+                    tma_load_3d(dst + chunk_bytes, &prm.tmap, &full_b[st], 0, (int32_t)(prm.s2_row0 + row0), 0);
+                } else {
+                    last_rec[st] = -1;   // no copy in flight
+                    mbar_arrive(&full_b[st]);
                 }
+            }
+            if (*abort) {
+                // let the copies in flight land before the CTA's shared memory goes
+                for (int st = 0; st < TC_NSB; ++st)
+                    if (last_rec[st] >= 0) {
+                        volatile int dummy = 0;
+                        mbar_wait(&full_b[st], ((uint32_t)last_rec[st] / TC_NSB) & 1u, &dummy, 100000000ull);
+                    }
+            }
         }
     } else if (warp == TC_MMA_WARP) {
         // ---------------- MMA issuer ----------------
