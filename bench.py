@@ -389,7 +389,9 @@ def simulator_leg(dev, seed: int = 7):
     return {"what": f"sim_us_rca: {n_ele}+{n_ele} RCA strips x {n_sub} sub-elements, {n_tx} plane waves, "
                     f"{n_scat} scatterers, {n_frame} frames, {p['n_freq']} frequencies, Raw {list(raw.shape)}",
             "ms": 1e3 * el, "element_field_terms_per_s": evals / el,
-            "note": "scatterers static within a frame: one element field per frame, all transmits as one GEMM"}
+            "note": "scatterers static within a frame: the frame's 16 transmits as one group; per group "
+                    "rcabf_sim_tx_field (fields summed over elements), rcabf_sim_rx_spectrum (summed over "
+                    "scatterers), rcabf_sim_rf (inverse transform at the kept samples); host set-up included"}
 
 
 WORKLOAD_KIND = {"c0": "single volume, 64+64 probe", "c1": "row + column transmits compounded, 128+128 probe",

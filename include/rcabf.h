@@ -402,6 +402,47 @@ int rcabf_sim_element_field(void *out, const float *r_scat, const float *r_ele, 
                             float height, float rfocus, int baffle, float lens, float speed_of_sound,
                             int64_t n_scat, int64_t n_ele, int64_t n_f, int64_t n_sub, void *stream);
 
+/* Transmit field of a group of n_tx transmit events that share scatterer
+ * positions (n_tx <= 16):
+ *   tx_out[f][s][g] = tx_factor[f] bsc[g][s]
+ *                     sum_e E(f, s, e) apod[g][e] exp(i w_f delay[g][e])
+ * with E the element field above (evaluated in place, not stored),
+ * w_f = Re(kwave[f]) speed_of_sound, delay in seconds relative to the
+ * receive start, tx_factor the conjugated pulse and transmit impulse-response
+ * spectra.  tx_out: device complex64 [n_f][n_scat][n_tx]; bsc, delay, apod:
+ * device float [n_tx][n_scat], [n_tx][n_ele], [n_tx][n_ele]; tx_factor:
+ * device complex64 [n_f]; n_ele * n_tx <= 4096.  Replaces the reference
+ * kernel TXfield and its backscatter product
+ * (MATLAB/lib/simulator/SimUS_CUDARCA.cu:209-292, SimUS_CUDARCA.m:319-344). */
+int rcabf_sim_tx_field(void *tx_out, const float *r_scat, const float *bsc, const float *r_ele, const void *kwave,
+                       const void *tx_factor, const float *delay, const float *apod, int64_t n_tx, float width,
+                       float height, float rfocus, int baffle, float lens, float speed_of_sound, int64_t n_scat,
+                       int64_t n_ele, int64_t n_f, int64_t n_sub, void *stream);
+/* Received spectrum of the same group:
+ *   spec_out[f][e][g] = rx_factor[f] apod[g][e] sum_s E_rx(f, s, e) tx_field[f][s][g]
+ * with E_rx the receive array's element field (evaluated in place) and
+ * rx_factor the input-filter x receive impulse-response spectrum.
+ * spec_out: device complex64 [n_f][n_ele][n_tx]; tx_field: the output of
+ * rcabf_sim_tx_field; apod: device float [n_tx][n_ele].  Replaces the
+ * reference kernel RXfield, the receive apodisation and the sum over
+ * scatterers (SimUS_CUDARCA.cu:294-379, SimUS_CUDARCA.m:346-372). */
+int rcabf_sim_rx_spectrum(void *spec_out, const void *tx_field, const float *r_scat, const float *r_ele,
+                          const void *kwave, const void *rx_factor, const float *apod, int64_t n_tx, float width,
+                          float height, float rfocus, int baffle, float lens, float speed_of_sound, int64_t n_scat,
+                          int64_t n_ele, int64_t n_f, int64_t n_sub, void *stream);
+/* Time-domain samples of the group's signals: with
+ *   RF(t, e, g) = Re(ifft(conj(spec[:, e, g]), n_fast))(t)
+ *              = (1 / n_fast) sum_f Re(spec[f][e][g] conj(twiddle[f t mod n_fast])) ,
+ * twiddle[m] = exp(2 pi i m / n_fast) (device complex64 [n_fast]),
+ * out[g][e][i] (device float [n_tx][n_ele][n_out]) holds RF(t(i)) with
+ * t(i) = i for sub = 0 (the RF, zero at t >= n_fast), and for sub > 0
+ * t(i) = sub (i / 2) + i mod 2: the interleave of RF(1:sub:end) and
+ * RF(2:sub:end) that the reference returns as Raw.  n_f * 8 <= 49152.
+ * Replaces the inverse FFT, crop / pad and sub-sampling of
+ * SimUS_CUDARCA.m:374-389. */
+int rcabf_sim_rf(float *out, const void *spec, const void *twiddle, int64_t n_f, int64_t n_ele, int64_t n_tx,
+                 int64_t n_fast, int32_t sub, int64_t n_out, void *stream);
+
 /* ------------------------------------------------------------------------ */
 /* ULM super-localisation (downstream of the clutter filter)                 */
 /* ------------------------------------------------------------------------ */

@@ -143,6 +143,14 @@ _SIGS = {
     "rcabf_sim_element_field": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                           C.c_float, C.c_int, C.c_float, C.c_float, C.c_int64, C.c_int64,
                                           C.c_int64, C.c_int64, C.c_void_p]),
+    "rcabf_sim_tx_field": (C.c_int, [C.c_void_p] * 8 + [C.c_int64, C.c_float, C.c_float, C.c_float, C.c_int,
+                                                        C.c_float, C.c_float, C.c_int64, C.c_int64, C.c_int64,
+                                                        C.c_int64, C.c_void_p]),
+    "rcabf_sim_rx_spectrum": (C.c_int, [C.c_void_p] * 7 + [C.c_int64, C.c_float, C.c_float, C.c_float, C.c_int,
+                                                           C.c_float, C.c_float, C.c_int64, C.c_int64, C.c_int64,
+                                                           C.c_int64, C.c_void_p]),
+    "rcabf_sim_rf": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                               C.c_int32, C.c_int64, C.c_void_p]),
     "rcabf_ulm_psf_corr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_int64, C.c_int64,
                                      C.c_int64, C.c_int32, C.c_int32, C.c_void_p]),
     "rcabf_ulm_ensemble": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int64, C.c_int64,

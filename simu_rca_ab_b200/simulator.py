@@ -9,15 +9,18 @@ For each frame (nTX consecutive events) and each transmit event:
   S(f, e')     = IPFilt(f) IRrx(f) a'_e' sum_s E_rx(f, s, e') TX(f, s)
   RF(:, e')   += real(ifft(conj(S(:, e')), nFastTime))
 
-with E the element field (librcabf ``rcabf_sim_element_field``: Green's
-function, directivities, lens phase), d / a the transmit delays and
-apodisation, a' the receive apodisation, P / IR / IPFilt the spectra of the
-pulse, impulse responses and input filter (SimUS_CUDARCA.m:111-246, 254-322).
-The element field is evaluated once per event (once per frame when all its
-events share scatterer positions); the sums over elements and scatterers are
-batched complex GEMMs over frequency (cuBLAS), the inverse transforms cuFFT.
+with E the element field (Green's function, directivities, lens phase), d /
+a the transmit delays and apodisation, a' the receive apodisation, P / IR /
+IPFilt the spectra of the pulse, impulse responses and input filter
+(SimUS_CUDARCA.m:111-246, 254-322).  Three librcabf kernels per group of
+events that share scatterer positions (a whole frame when the scatterers do
+not move between its events, else one event), up to 16 transmits at a time:
+``rcabf_sim_tx_field`` (TX, the element field evaluated in the sum over
+elements), ``rcabf_sim_rx_spectrum`` (S, the receive field evaluated in the
+sum over scatterers) and ``rcabf_sim_rf`` (the inverse transform as a direct
+sum over the frequencies, evaluated only at the samples the output keeps).
 The output Raw interleaves RF(1:sub:end) and RF(2:sub:end) as the reference
-does (SimUS_CUDARCA.m:338-339), the quadrature-sampled layout the
+does (SimUS_CUDARCA.m:385-386), the quadrature-sampled layout the
 beamformer's real-input path reads.
 """
 from __future__ import annotations
@@ -31,6 +34,7 @@ import torch
 from . import _lib as L
 
 SIM_FS = 250e6      # sampling rate of pulse shapes and impulse responses (SimUS_CUDARCA.m:101)
+SIM_GMAX = 16       # transmits one rcabf_sim_tx_field / rcabf_sim_rx_spectrum call takes
 SUB = {"NS200BW": 2, "BS100BW": 4, "BS50BW": 8}
 
 
@@ -111,6 +115,18 @@ def _element_field(dev, r_scat, ele, k, trans, c, stream):
     return out
 
 
+def _props(trans):
+    return (float(np.ravel(trans["ElementWidth"])[0]), float(np.ravel(trans["ElementHeight"])[0]),
+            float(np.ravel(trans["ElementElevationFocus"])[0]), int(np.ravel(trans["baffle"])[0]),
+            float(trans["lensCorrection"]))
+
+
+def _out_samples(numel: int, sub: int) -> int:
+    """Length of Raw along fast time: the interleave of RF(1:sub:end) and
+    RF(2:sub:end), each cut to the shorter of the two."""
+    return 2 * min(-(-numel // sub), -(-(numel - 1) // sub))
+
+
 def sim_us_rca(Media, TransTX, TransRX, TXSI, RXSI, Options=None, *, device=None, return_rf: bool = False):
     """Simulated raw channel data [fast time (I/Q interleaved), element, event]
     (float32 numpy, SimUS_CUDARCA.m's Raw); ``return_rf`` also returns the RF
@@ -120,53 +136,67 @@ def sim_us_rca(Media, TransTX, TransRX, TXSI, RXSI, Options=None, *, device=None
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else torch.device(device).index or 0)
     p = sim_plan(Media, TransTX, TransRX, TXSI, RXSI)
     n_tx, n_f, n_fast = p["n_tx"], p["n_freq"], p["n_fast"]
-    cplx = lambda a: torch.from_numpy(np.asarray(a, np.complex64)).to(dev)
+    cplx = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.complex64)).to(dev)
+    flt = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
     k = cplx(p["k"])
-    w = torch.from_numpy(np.real(p["k"]).astype(np.float32) * np.float32(p["c"])).to(dev)     # angular frequency
-    tx_fac = (cplx(p["pulse"]).conj() * cplx(p["ir_tx"]).conj())                               # [f]
-    rx_fac = cplx(p["ipf"]) * cplx(p["ir_rx"])                                                  # [f]
-    delay = torch.from_numpy(p["delay"].astype(np.float32)).to(dev)                           # [e, tx]
-    apod = torch.from_numpy(p["apod"].astype(np.float32)).to(dev)
-    # transmit weights W[f][e][tx] = apod exp(i w (delay - t_rx))
-    wtx = apod[None] * torch.polar(torch.ones_like(delay)[None].expand(n_f, -1, -1),
-                                   w[:, None, None] * delay[None])
-    rx_apod = torch.from_numpy(p["rx_apod"].astype(np.float32)).to(dev)                       # [e', tx]
+    tx_fac = cplx(np.conj(p["pulse"]) * np.conj(p["ir_tx"]))                                  # [f]
+    rx_fac = cplx(p["ipf"] * p["ir_rx"])                                                      # [f]
+    delay = p["delay"].astype(np.float32)                                                     # [e, tx]
+    apod = p["apod"].astype(np.float32)
+    rx_apod = p["rx_apod"].astype(np.float32)                                                 # [e', tx]
     ele_tx = torch.from_numpy(_ele_layout(p["pos_tx"])).to(dev)
     ele_rx = torch.from_numpy(_ele_layout(p["pos_rx"])).to(dev)
     n_ele_rx = p["pos_rx"].shape[0]
+    n_ele_tx, n_sub_tx, n_sub_rx = p["pos_tx"].shape[0], p["pos_tx"].shape[2], p["pos_rx"].shape[2]
+    twiddle = cplx(np.exp(2j * np.pi * np.arange(n_fast) / n_fast))
     scat = p["scat"]
     n_event = p["n_event"]
-    rf = torch.zeros((n_event, n_ele_rx, n_fast), dtype=torch.float32, device=dev)
+    numel, sub = p["numel"], p["sub"]
+    n_out = _out_samples(numel, sub)
+    raw = torch.empty((n_event, n_ele_rx, n_out), dtype=torch.float32, device=dev)
+    rf = torch.empty((n_event, n_ele_rx, numel), dtype=torch.float32, device=dev) if return_rf else None
     stream = torch.cuda.current_stream(dev).cuda_stream
-    prev = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
-    try:
-        for frame in range(n_event // n_tx):
-            ev = list(range(frame * n_tx, (frame + 1) * n_tx))
-            pos = scat[:, :3, ev]                     # [s, 3, tx]
-            bsc = torch.from_numpy(scat[:, 3, ev].astype(np.float32)).to(dev)   # [s, tx]
-            same = all(np.array_equal(pos[:, :, 0], pos[:, :, j]) for j in range(1, n_tx))
-            groups = [list(range(n_tx))] if same else [[j] for j in range(n_tx)]
-            for grp in groups:
-                r = torch.from_numpy(np.ascontiguousarray(pos[:, :, grp[0]].T, dtype=np.float32)).to(dev)
-                e_tx = _element_field(dev, r, ele_tx, k, p["tx"], p["c"], stream)      # [f, s, e]
-                e_rx = _element_field(dev, r, ele_rx, k, p["rx"], p["c"], stream)      # [f, s, e']
-                idx = torch.as_tensor(grp, device=dev)
-                txf = torch.bmm(e_tx, wtx[:, :, idx])                                 # [f, s, g]
-                txf = txf * tx_fac[:, None, None] * bsc[None, :, idx]
-                spec = torch.bmm(e_rx.transpose(1, 2), txf)                           # [f, e', g]
-                spec = spec * rx_fac[:, None, None] * rx_apod[None, :, idx]
-                sig = torch.fft.ifft(spec.conj(), n=n_fast, dim=0).real              # [t, e', g]
-                rf[[ev[j] for j in grp]] += sig.permute(2, 1, 0)
-    finally:
-        torch.backends.cuda.matmul.allow_tf32 = prev
-    n = p["numel"]
-    rf = rf[:, :, :n] if n_fast >= n else torch.nn.functional.pad(rf, (0, n - n_fast))
-    sub = p["sub"]
-    a = rf[:, :, 0::sub]
-    b = rf[:, :, 1::sub]
-    m = min(a.shape[2], b.shape[2])
-    raw = torch.stack([a[:, :, :m], b[:, :, :m]], dim=3).reshape(n_event, n_ele_rx, 2 * m)
+    lib = L.lib()
+    ptx, prx = _props(p["tx"]), _props(p["rx"])
+    c = float(p["c"])
+    for frame in range(n_event // n_tx):
+        ev = list(range(frame * n_tx, (frame + 1) * n_tx))
+        pos = scat[:, :3, ev]                     # [s, 3, tx]
+        n_scat = pos.shape[0]
+        same = all(np.array_equal(pos[:, :, 0], pos[:, :, j]) for j in range(1, n_tx))
+        groups = [list(range(n_tx))] if same else [[j] for j in range(n_tx)]
+        groups = [g[i:i + SIM_GMAX] for g in groups for i in range(0, len(g), SIM_GMAX)]
+        for grp in groups:
+            G = len(grp)
+            r = flt(pos[:, :, grp[0]].T)                                      # [3][s]
+            bsc = flt(scat[:, 3, [ev[j] for j in grp]].T)                    # [g][s]
+            d = flt(delay[:, grp].T)                                          # [g][e]
+            a = flt(apod[:, grp].T)
+            ra = flt(rx_apod[:, grp].T)                                       # [g][e']
+            txf = torch.empty((n_f, n_scat, G), dtype=torch.complex64, device=dev)
+            L.check(lib.rcabf_sim_tx_field(
+                C.c_void_p(txf.data_ptr()), C.c_void_p(r.data_ptr()), C.c_void_p(bsc.data_ptr()),
+                C.c_void_p(ele_tx.data_ptr()), C.c_void_p(k.data_ptr()), C.c_void_p(tx_fac.data_ptr()),
+                C.c_void_p(d.data_ptr()), C.c_void_p(a.data_ptr()), G, *ptx[:4], ptx[4], c, n_scat, n_ele_tx, n_f,
+                n_sub_tx, C.c_void_p(stream)), "rcabf_sim_tx_field")
+            spec = torch.empty((n_f, n_ele_rx, G), dtype=torch.complex64, device=dev)
+            L.check(lib.rcabf_sim_rx_spectrum(
+                C.c_void_p(spec.data_ptr()), C.c_void_p(txf.data_ptr()), C.c_void_p(r.data_ptr()),
+                C.c_void_p(ele_rx.data_ptr()), C.c_void_p(k.data_ptr()), C.c_void_p(rx_fac.data_ptr()),
+                C.c_void_p(ra.data_ptr()), G, *prx[:4], prx[4], c, n_scat, n_ele_rx, n_f, n_sub_rx,
+                C.c_void_p(stream)), "rcabf_sim_rx_spectrum")
+            evs = [ev[j] for j in grp]
+            e0, e1 = evs[0], evs[-1] + 1
+            contiguous = evs == list(range(e0, e1))
+            for buf, sb, n in ((raw, sub, n_out), (rf, 0, numel)):
+                if buf is None:
+                    continue
+                dst = buf[e0:e1] if contiguous else torch.empty((G, n_ele_rx, n), dtype=torch.float32, device=dev)
+                L.check(lib.rcabf_sim_rf(C.c_void_p(dst.data_ptr()), C.c_void_p(spec.data_ptr()),
+                                         C.c_void_p(twiddle.data_ptr()), n_f, n_ele_rx, G, n_fast, sb, n,
+                                         C.c_void_p(stream)), "rcabf_sim_rf")
+                if not contiguous:
+                    buf[evs] = dst
     raw_np = raw.permute(2, 1, 0).cpu().numpy()          # [fast time, element, event]
     if return_rf:
         return raw_np, rf.permute(2, 1, 0).cpu().numpy()

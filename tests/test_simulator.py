@@ -8,8 +8,10 @@ the transmit delay / apodisation / pulse / impulse responses as the product
 combines them, reproduces the reference kernels TXfield and RXfield compiled
 for sm_100a (O2, no fast math) and for the host (O1) within 1e-4 relative
 RMS, with a flat and with a focused elevation aperture; the whole simulation
-(frames, events, sums, inverse transforms, sub-sampling) reproduces the
-reference pipeline run with the O1 kernels within 1e-4.
+(frames, events, the fields evaluated inside the transmit and receive sums,
+the inverse transforms as direct sums, sub-sampling: rcabf_sim_tx_field,
+rcabf_sim_rx_spectrum, rcabf_sim_rf) reproduces the reference pipeline run
+with the O1 kernels within 1e-4.
 """
 import numpy as np
 import pytest
@@ -117,14 +119,16 @@ def test_element_field_reproduces_the_reference_kernels(cuda, focus, baffle):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not OS.have_sim_cpu(), reason="oracle/_ref simulator build missing")
-@pytest.mark.parametrize("moving", [True, False])
-def test_simulation_matches_the_reference_pipeline(cuda, moving):
+@pytest.mark.parametrize("moving,n_tx", [(True, 2), (False, 2), (False, 18)])
+def test_simulation_matches_the_reference_pipeline(cuda, moving, n_tx):
+    """Moving scatterers (one group per event), static ones (the frame's
+    events as one group) and 18 transmits (groups of 16 and 2)."""
     from simu_rca_ab_b200.simulator import sim_us_rca
-    case = sim_case(moving=moving)
+    case = sim_case(moving=moving, n_tx=n_tx)
     raw, rf = sim_us_rca(*case, return_rf=True)
     raw_ref, rf_ref = OS.simulate(OS.plan(*case))
     assert raw.shape == raw_ref.shape
     e = _rel(raw, raw_ref)
-    print(f"simulation (moving={moving}): Raw {e:.2e} rel RMS vs the reference pipeline (O1 kernels)")
+    print(f"simulation (moving={moving}, {n_tx} tx): Raw {e:.2e} rel RMS vs the reference pipeline (O1 kernels)")
     assert e < 1e-4
     assert _rel(rf, rf_ref) < 1e-4
