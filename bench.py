@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-clutter", action="store_true", help="skip the SVD clutter filter of the ensemble")
     ap.add_argument("--no-simulator", action="store_true", help="skip the simulator timing")
     ap.add_argument("--no-ulm", action="store_true", help="skip the ULM super-localisation timing")
+    ap.add_argument("--no-per-channel", action="store_true", help="skip the no-sum (per-channel) timing")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-rates", default="6,60", help="c3 Poisson arrival rates (requests/s), comma-separated")
     ap.add_argument("--no-serving-plain", action="store_true", help="skip serving the stream on the plain kernel")
@@ -392,6 +393,56 @@ def simulator_leg(dev, seed: int = 7):
             "note": "scatterers static within a frame: the frame's 16 transmits as one group; per group "
                     "rcabf_sim_tx_field (fields summed over elements), rcabf_sim_rx_spectrum (summed over "
                     "scatterers), rcabf_sim_rf (inverse transform at the kept samples); host set-up included"}
+
+
+def per_channel_leg(eng, dev, n_frame: int = 100):
+    """The no-sum beamformer (bf_rca_nosum, the reference's
+    bfVirtualSourceGeneric_RCA_Nosum) as the dataset producer calls it
+    (MATLAB/save_simus_sh.m:354-393): one value per receive element on a
+    1 x 1 x 17 line of depths, here on the 64+64 probe of the single-volume
+    workload with its 16 transmits and n_frame frames of channel data
+    resident.  Times every frame in one launch (the planner's choice) against
+    one launch per frame (the plain kernel by name); the outputs are compared
+    bit for bit."""
+    import numpy as np
+    import torch
+
+    from simu_rca_ab_b200 import _lib as L
+    from simu_rca_ab_b200 import workloads as W
+    from simu_rca_ab_b200.params import normalize
+    w = W.get("c0", n_frame=n_frame)
+    g = w.groups[0]
+    G = dict(g.Geometry)
+    z = np.linspace(5e-3, 25e-3, 17).reshape(17, 1, 1)
+    G.update(gridBfX=np.zeros_like(z), gridBfY=np.zeros_like(z), gridBfZ=z)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        geom = eng.geometry(normalize(np.zeros(1, np.complex64), G, g.Transmit, w.Param, w.Options))
+    iq = W.group_data(w, W.channel_data(w, seed=3, device=dev), 0).contiguous()
+    outs = {}
+    times = {}
+    for name, kern in (("all_frames", L.KERNEL_AUTO), ("per_frame", L.KERNEL_PLAIN)):
+        out = torch.empty((geom.n_ele, n_frame, geom.n_tx, geom.n_pix), dtype=torch.complex64, device=dev)
+        a = eng.make_args(geom, iq, iq_dtype=L.IQ_C64, n_sample=w.n_sample, n_frame=n_frame, out=out, mask=None,
+                          compound=False, storage=L.STORE_F32, kernel=kern, per_channel=True)
+        for _ in range(2):
+            eng.run(geom, a)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            eng.run(geom, a)
+        e1.record()
+        torch.cuda.synchronize()
+        times[name] = e0.elapsed_time(e1) / reps
+        outs[name] = out
+    return {"what": f"bf_rca_nosum: 64+64 probe, 16 transmits, 64 receive elements, {n_frame} frames, 1x1x17 "
+                    f"depths; output [element][frame][tx][pixel]",
+            "all_frames_ms": times["all_frames"], "per_frame_launches_ms": times["per_frame"],
+            "speedup": times["per_frame"] / times["all_frames"],
+            "identical": bool(torch.equal(outs["all_frames"], outs["per_frame"]))}
 
 
 WORKLOAD_KIND = {"c0": "single volume, 64+64 probe", "c1": "row + column transmits compounded, 128+128 probe",
@@ -890,6 +941,13 @@ def main():
         except Exception as ex:
             sim = {"error": f"{type(ex).__name__}: {ex}"}
 
+    per_ch = None
+    if not a.no_per_channel and rank == 0:
+        try:
+            per_ch = per_channel_leg(eng, dev)
+        except Exception as ex:
+            per_ch = {"error": f"{type(ex).__name__}: {ex}"}
+
     ulm = None
     if not a.no_ulm and rank == 0:
         try:
@@ -972,7 +1030,7 @@ def main():
                        "plan": plan, "autotune": tune},
             "latency": {"p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "stage_ms": stage_ms, "roofline": roof, "cpu_baseline": cb, "e2e": e2e, "plain_kernel": plain, "reference_gpu": ref_gpu,
-            "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim, "ulm": ulm,
+            "serving": serving, "graph": graph, "clutter_filter": clutter, "simulator": sim, "per_channel": per_ch, "ulm": ulm,
             "tensor_core_fp16_weights": tc16,
             "gpu_launches": int(launches.value), "clocks": clk, "accuracy": acc,
         }

@@ -431,8 +431,11 @@ def bf_rca_nosum(data, Geometry, Transmit, Param, Options=None, *, engine: Engin
     T = geom.n_tx
     out = torch.empty((geom.n_ele, n_frame, T, geom.n_pix), dtype=torch.complex64, device=eng.device)
     mask = torch.empty((T, geom.n_pix), dtype=torch.float32, device=eng.device)
+    # every frame in one launch (pc_das_kernel); Options.kernel = 'plain'
+    # keeps the one-launch-per-frame kernel
+    kern = L.KERNEL_PLAIN if acq.kernel == L.KERNEL_PLAIN else L.KERNEL_AUTO
     a = eng.make_args(geom, t, iq_dtype=iq_dtype, n_sample=n_sample, n_frame=n_frame, out=out, mask=mask,
-                      compound=False, storage=acq.storage, kernel=L.KERNEL_PLAIN, per_channel=True)
+                      compound=False, storage=acq.storage, kernel=kern, per_channel=True)
     eng.run(geom, a, stream=stream)
     s1, s2, s3 = acq.grid.shape
     dataBf = out.view(geom.n_ele, n_frame, T, s3, s2, s1).permute(5, 4, 3, 2, 1, 0)

@@ -149,6 +149,9 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     p = Plan{};
     p.kernel = (a->kernel == RCABF_KERNEL_PLAIN || a->per_channel) ? RCABF_KERNEL_PLAIN : RCABF_KERNEL_FUSED;
     if (p.kernel == RCABF_KERNEL_PLAIN) {
+        // per-channel output: all frames in one launch unless the
+        // one-launch-per-frame kernel is asked for by name
+        p.pc_all = a->per_channel && a->kernel != RCABF_KERNEL_PLAIN ? 1 : 0;
         p.total = 0;
         return RCABF_OK;
     }
@@ -460,7 +463,13 @@ static int beamform_planned(rcabf_geometry *g, const rcabf_beamform_args *a, con
         pp.per_channel = a->per_channel ? 1 : 0;
         pp.out = reinterpret_cast<float2 *>(a->out);
         pp.err_count = device_state(g->device)->err;
-        for (int64_t f = 0; f < a->n_frame; ++f) {
+        if (p.pc_all) {
+            pp.frame = -1;   // every frame
+            const cudaError_t le = launch_plain(g->mode, g->kind, pp, st);
+            if (le != cudaSuccess) return cuda_fail(le, "per-channel kernel launch");
+            g_launches += 1;
+        }
+        for (int64_t f = 0; f < a->n_frame && !p.pc_all; ++f) {
             pp.frame = f;
             const cudaError_t le = launch_plain(g->mode, g->kind, pp, st);
             if (le != cudaSuccess) return cuda_fail(le, "plain kernel launch");
@@ -676,7 +685,8 @@ int rcabf_describe_plan(const rcabf_geometry *g, const rcabf_beamform_args *a, c
         s = resident_ctas(g, p, p.smem, device_state(g->device), occ);
         if (s != RCABF_OK) return s;
     }
-    const char *kname = p.kernel == RCABF_KERNEL_PLAIN ? "plain"
+    const char *kname = p.pc_all                         ? "per_channel_all_frames"
+                        : p.kernel == RCABF_KERNEL_PLAIN ? "plain"
                         : p.tc == 2                     ? "fused_tensor_core"
                         : p.tc == 1                     ? "fused_tensor_core_fp16w"
                         : p.vb == 2                     ? "fused_voxel_blocked_tmem"

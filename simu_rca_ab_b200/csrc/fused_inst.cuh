@@ -48,7 +48,13 @@ template <int MODE, int KIND, int IQ>
 static cudaError_t plain_do(const PlainParams &p, cudaStream_t st)
 {
     const int64_t n = p.g.n_z * p.g.n_u * p.g.n_v;
-    if (p.per_channel)
+    if (p.per_channel && p.frame < 0) {   // every frame in one launch
+        int dev = 0, n_sm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t blocks = std::min<int64_t>((n * p.g.n_ele + 255) / 256, (int64_t)n_sm * 16);
+        pc_das_kernel<MODE, KIND, IQ><<<(unsigned)blocks, 256, 0, st>>>(p);
+    } else if (p.per_channel)
         plain_das_kernel<MODE, KIND, IQ, true><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);
     else
         plain_das_kernel<MODE, KIND, IQ, false><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p);

@@ -132,4 +132,78 @@ __global__ void __launch_bounds__(256) plain_das_kernel(const __grid_constant__ 
     }
 }
 
+// Per-channel output (the reference's no-sum kernels) over all frames in one
+// launch: one thread per (voxel, receive element), voxels fastest so that a
+// warp's writes of one (element, frame, transmit) are contiguous; each
+// (transmit, element) setup -- delays, weights, phasor, masks -- is formed
+// once and serves every frame.  Per (voxel, element, transmit, frame) the
+// arithmetic is the PC plain kernel's, in its order: the same bits, from one
+// launch instead of one per frame.
+template <int MODE, int KIND, int IQ>
+__global__ void __launch_bounds__(256) pc_das_kernel(const __grid_constant__ PlainParams prm)
+{
+    using KT = KindTraits<KIND>;
+    const DevGeom &g = prm.g;
+    const int64_t n_vox = g.n_z * g.n_u * g.n_v;
+    const int64_t n_rxkey = g.n_u * g.n_z, n_txkey = g.n_v * g.n_z;
+    const int64_t n = n_vox * g.n_ele;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = i % n_vox;
+        const int rx = (int)(i / n_vox);
+        const int64_t iz = v % g.n_z;
+        const int64_t iu = (v / g.n_z) % g.n_u;
+        const int64_t iv = v / (g.n_z * g.n_u);
+        const int64_t rxkey = iu * g.n_z + iz, txkey = iv * g.n_z + iz;
+        const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
+        for (int tx = 0; tx < g.n_tx; ++tx) {
+            const float4 t = __ldg(&g.tx_tab[(int64_t)tx * n_txkey + txkey]);
+            bool ok = ((MODE == MODE_EXACT) ? t.w : t.y) != 0.0f;
+            if (g.cone_u != nullptr) ok = ok && g.cone_u[(int64_t)tx * n_rxkey + rxkey] != 0;
+            Setup<KIND> st;
+            if (ok) {
+                const float4 e = __ldg(&g.rx_tab[(int64_t)rx * n_rxkey + rxkey]);
+                const float ab = ab_value(g, tx, rx);
+                if constexpr (MODE == MODE_EXACT)
+                    setup_exact<KIND>(t, e, ab, ab_phasor(g, tx, rx), prm.n_sample, st);
+                else
+                    setup_ref<KIND>(t, e, ab, g.ref, prm.n_sample, st);
+                ok = st.ok;
+            }
+            for (int64_t f = 0; f < prm.n_frame; ++f) {
+                float2 *o = prm.out + (((int64_t)rx * prm.n_frame + f) * g.n_tx + tx) * g.n_pix + pix;
+                if (!ok) {
+                    if (!prm.accumulate) *o = make_float2(0.f, 0.f);
+                    continue;
+                }
+                const int64_t base = ((f * g.n_tx + tx) * (int64_t)g.n_ele + rx) * prm.n_sample + st.n0 - KT::LO;
+                float2 tsum = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < KT::TAPS; ++j) {
+                    const float2 x = load_iq<IQ>(prm.iq, base + j);
+                    if constexpr (MODE == MODE_EXACT) {
+                        tsum.x = fmaf(st.w[j], x.x, tsum.x);
+                        tsum.y = fmaf(st.w[j], x.y, tsum.y);
+                    } else if (j == 0) {
+                        tsum = make_float2(__fmul_rn(st.w[0], x.x), __fmul_rn(st.w[0], x.y));
+                    } else {
+                        tsum.x = __fadd_rn(tsum.x, __fmul_rn(st.w[j], x.x));
+                        tsum.y = __fadd_rn(tsum.y, __fmul_rn(st.w[j], x.y));
+                    }
+                }
+                float2 term;
+                if constexpr (MODE == MODE_EXACT) {
+                    term.x = fmaf(st.P.x, tsum.x, -st.P.y * tsum.y);
+                    term.y = fmaf(st.P.x, tsum.y, st.P.y * tsum.x);
+                } else {
+                    const float cs = st.P.x, sn = st.P.y;
+                    term.x = __fmul_rn(st.apod, __fadd_rn(__fmul_rn(tsum.x, cs), __fmul_rn(tsum.y, sn)));
+                    term.y = __fmul_rn(st.apod, __fadd_rn(__fmul_rn(-tsum.x, sn), __fmul_rn(tsum.y, cs)));
+                }
+                if (prm.accumulate) { float2 q = *o; q.x += term.x; q.y += term.y; *o = q; }
+                else *o = term;
+            }
+        }
+    }
+}
+
 }  // namespace rcabf

@@ -14,6 +14,7 @@ constexpr size_t SMEM_BUDGET = 110 * 1024;
 
 struct Plan {
     int kernel = 0;       // rcabf_kernel
+    int pc_all = 0;       // per-channel output, every frame in one launch (pc_das_kernel)
     int vb = 0;           // voxel-blocked kernel (fused_vb_kernel.cuh): 1 register, 2 TMEM accumulators
     int tc = 0;           // tensor-core kernel (fused_tc_kernel.cuh): 1 FP16 weights, 2 hi + remainder weights
     int tc_rows = 0;      // its slab rows (the record + zero rows a window may reach past it)

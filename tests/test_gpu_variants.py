@@ -102,3 +102,29 @@ def test_per_channel_terms_sum_to_the_beamformed_volume(bf):
         summed, _ = bf.bf_rca(data, G, T, P, {**O, "flagCompounding": False, "tableMode": "exact",
                                                 "kernel": "plain"})
     assert H.rel_rms(per.sum(axis=-1), summed) < 1e-5
+
+
+@pytest.mark.parametrize("table_mode", ["ref_compat", "exact"])
+@pytest.mark.parametrize("name", ["nosumab_ref6_rx_y", "nosum_quad3_rx_x_mask"])
+def test_per_channel_all_frames_launch_gives_the_per_frame_kernels_bits(bf, name, table_mode):
+    """The per-channel output of every frame from one launch (pc_das_kernel,
+    the planner's choice) against the one-launch-per-frame kernel (by name):
+    identical bits on ten frames (the fixture's events repeated at five
+    scales), with an aberration law and with the cone mask, in both table
+    modes."""
+    data, G, T, P, O, outs = load(name)
+    ab = outs.get("ab_law")
+    P2 = dict(P)
+    if ab is not None:
+        P2["AbLawRx"] = _param_law(ab)
+    d5 = np.concatenate([data * (1.0 + 0.25 * f) for f in range(5)], axis=-1)   # events axis
+    opts = {**O, "flagCompounding": False, "tableMode": table_mode}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        one, m1 = bf.bf_rca_nosum(d5, G, T, P2, opts)
+        per, m2 = bf.bf_rca_nosum(d5, G, T, P2, {**opts, "kernel": "plain"})
+        single, _ = bf.bf_rca_nosum(data, G, T, P2, opts)
+    assert one.shape == per.shape and one.shape[-2] == 5 * single.shape[-2]
+    assert np.array_equal(one, per)
+    assert np.array_equal(m1, m2)
+    assert np.abs(one).max() > 0
