@@ -190,7 +190,8 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
         p.n_items = (int64_t)p.n_fb * p.tiles_z * p.tiles_u * p.tiles_v;
     };
 
-    // Tensor-core kernel: FP16 slabs, exact tables, compounded output, a
+    // Tensor-core kernel: FP16 slabs (BF16 slabs with hi + remainder weights),
+    // exact tables, compounded output, a
     // rectilinear grid whose 4 x 32 x 1 tiles need windows of at most 32
     // rows, at least 32 frames; frame blocks of a multiple of 8 frames, as
     // few as the tensor-memory budget allows (the weights are built once
@@ -208,7 +209,8 @@ int plan_beamform(rcabf_geometry *g, const rcabf_beamform_args *a, Plan &p, cons
     const int want_tc = named_tc ? named_tc : auto_tc ? 2 : 0;
     if (want_tc) {
         const int fbmax = tc_max_frames_per_block(want_tc == 2);
-        bool ok = g->mode == MODE_EXACT && a->storage == RCABF_STORE_F16 && a->compound && !a->per_channel &&
+        const bool store_ok = a->storage == RCABF_STORE_F16 || (a->storage == RCABF_STORE_BF16 && want_tc == 2);
+        bool ok = g->mode == MODE_EXACT && store_ok && a->compound && !a->per_channel &&
                   g->grid_kind == RCABF_GRID_RECTILINEAR && a->n_sample >= 2;
         // the 128-voxel tile whose windows are shortest (a forced shape if given)
         TileShape tts{TC_TILE_U, TC_TILE_V, 1};
@@ -404,7 +406,7 @@ int launch_fused_jobs(rcabf_geometry *g0, FusedParams &prm, const Plan &p, cudaS
     if (p.tc) {   // one launch per job (a persistent grid of one CTA per SM each)
         for (int j = 0; j < prm.n_jobs; ++j) {
             const int64_t end = j + 1 < prm.n_jobs ? prm.jobs[j + 1].item_begin : prm.n_items;
-            const cudaError_t le = launch_fused_tc(g0->kind, p.tc == 2, prm.jobs[j], p.fb, p.tc_rows,
+            const cudaError_t le = launch_fused_tc(g0->kind, p.tc == 2, p.store == ST_BF16, prm.jobs[j], p.fb, p.tc_rows,
                                                    end - prm.jobs[j].item_begin, prm.err_count, ds->n_sm, st);
             if (le != cudaSuccess) return cuda_fail(le, "tensor-core kernel launch");
             g_launches += 1;

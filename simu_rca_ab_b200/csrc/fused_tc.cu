@@ -27,30 +27,33 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-template <int KIND, bool SPLIT>
+template <int KIND, bool SPLIT, bool BF>
 static cudaError_t tc_do(const TcParams *p, int grid, size_t smem, cudaStream_t st, int what)
 {
-    auto k = fused_tc_kernel<KIND, SPLIT>;
+    auto k = fused_tc_kernel<KIND, SPLIT, BF>;
     if (what == 1) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<grid, TC_THREADS, smem, st>>>(*p);
     return cudaGetLastError();
 }
 
+// FP16 slabs with either weight precision; BF16 slabs with hi + remainder
+// weights only
 template <int KIND>
-static cudaError_t tc_split(bool split, const TcParams *p, int grid, size_t smem, cudaStream_t st, int what)
+static cudaError_t tc_split(bool split, bool bf, const TcParams *p, int grid, size_t smem, cudaStream_t st, int what)
 {
-    return split ? tc_do<KIND, true>(p, grid, smem, st, what) : tc_do<KIND, false>(p, grid, smem, st, what);
+    if (bf) return split ? tc_do<KIND, true, true>(p, grid, smem, st, what) : cudaErrorInvalidValue;
+    return split ? tc_do<KIND, true, false>(p, grid, smem, st, what) : tc_do<KIND, false, false>(p, grid, smem, st, what);
 }
 
-static cudaError_t tc_route(int kind, bool split, const TcParams *p, int grid, size_t smem, cudaStream_t st,
+static cudaError_t tc_route(int kind, bool split, bool bf, const TcParams *p, int grid, size_t smem, cudaStream_t st,
                             int what)
 {
     switch (kind) {
-    case K_QUAD3: return tc_split<K_QUAD3>(split, p, grid, smem, st, what);
-    case K_REF6: return tc_split<K_REF6>(split, p, grid, smem, st, what);
-    case K_LANCZOS2: return tc_split<K_LANCZOS2>(split, p, grid, smem, st, what);
-    case K_LANCZOS3: return tc_split<K_LANCZOS3>(split, p, grid, smem, st, what);
-    case K_LANCZOS4: return tc_split<K_LANCZOS4>(split, p, grid, smem, st, what);
+    case K_QUAD3: return tc_split<K_QUAD3>(split, bf, p, grid, smem, st, what);
+    case K_REF6: return tc_split<K_REF6>(split, bf, p, grid, smem, st, what);
+    case K_LANCZOS2: return tc_split<K_LANCZOS2>(split, bf, p, grid, smem, st, what);
+    case K_LANCZOS3: return tc_split<K_LANCZOS3>(split, bf, p, grid, smem, st, what);
+    case K_LANCZOS4: return tc_split<K_LANCZOS4>(split, bf, p, grid, smem, st, what);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -65,9 +68,10 @@ size_t tc_launch_smem(int fb)
 int tc_max_frames_per_block(int split) { return tc_max_fb(split != 0); }
 int tc_tmem_columns(int fb, int split) { return tc_tmem_cols(fb, split != 0); }
 
-cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, int rows_per_slab, int64_t n_items,
-                            unsigned long long *err, int n_sm, cudaStream_t st)
+cudaError_t launch_fused_tc(int kind, int split, int bf16, const FusedJob &job, int fb, int rows_per_slab,
+                            int64_t n_items, unsigned long long *err, int n_sm, cudaStream_t st)
 {
+    if (bf16 && !split) return cudaErrorInvalidValue;
     if (fb < 32 || fb > tc_max_fb(split != 0) || (fb & 7) || tc_tmem_cols(fb, split != 0) > 512)
         return cudaErrorInvalidValue;
     const int64_t rows = (int64_t)job.g.n_tx * job.g.n_ele * job.n_fb * rows_per_slab;   // of each slab set
@@ -95,17 +99,17 @@ cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, in
     cuuint64_t strides[2] = {(cuuint64_t)(4 * fb), 128};
     cuuint32_t box[3] = {64, 16, (cuuint32_t)np};
     cuuint32_t es[3] = {1, 1, 1};
-    const CUresult cr = enc(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(job.S), dims, strides, box,
+    const CUresult cr = enc(&p.tmap, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(job.S), dims, strides, box,
                             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
     const size_t smem = tc_launch_smem(fb);
     if (job.g.mode != MODE_EXACT || !job.compound) return cudaErrorInvalidValue;
     cudaError_t e;
-    if ((e = tc_route(kind, split != 0, nullptr, 0, smem, nullptr, 1)) != cudaSuccess) return e;
+    if ((e = tc_route(kind, split != 0, bf16 != 0, nullptr, 0, smem, nullptr, 1)) != cudaSuccess) return e;
     const int grid = (int)std::min<int64_t>(n_items, n_sm);
     if (grid <= 0) return cudaSuccess;
-    return tc_route(kind, split != 0, &p, grid, smem, st, 0);
+    return tc_route(kind, split != 0, bf16 != 0, &p, grid, smem, st, 0);
 }
 
 }  // namespace rcabf

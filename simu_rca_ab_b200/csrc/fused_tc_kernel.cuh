@@ -200,21 +200,41 @@ __device__ __forceinline__ void tc_place(const float (&w)[TAPS], int o, float (&
     }
 }
 
-// FP32 values -> packed FP16 pairs (even index in the low half): the value's
-// rounding (hi) and, for SPLIT, the rounding of the remainder (lo).
+// FP32 values -> packed 16-bit pairs (even index in the low half), FP16 or
+// (BF) BF16, the operand type of the slabs: the value's rounding (hi) and,
+// for SPLIT, the rounding of the remainder (lo).
+template <bool BF>
 __device__ __forceinline__ uint32_t tc_pack(float a, float b)
 {
-    __half2 h = __floats2half2_rn(a, b);
-    return *reinterpret_cast<uint32_t *>(&h);
+    uint32_t r;
+    if constexpr (BF) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        memcpy(&r, &h, 4);
+    } else {
+        __half2 h = __floats2half2_rn(a, b);
+        memcpy(&r, &h, 4);
+    }
+    return r;
 }
+template <bool BF>
 __device__ __forceinline__ uint32_t tc_pack_rem(float a, float b, uint32_t hi)
 {
-    __half2 h = *reinterpret_cast<__half2 *>(&hi);
-    const float2 f = __half22float2(h);
-    return tc_pack(a - f.x, b - f.y);
+    float2 f;
+    if constexpr (BF) {
+        __nv_bfloat162 h;
+        memcpy(&h, &hi, 4);
+        f = __bfloat1622float2(h);
+    } else {
+        __half2 h;
+        memcpy(&h, &hi, 4);
+        f = __half22float2(h);
+    }
+    return tc_pack<BF>(a - f.x, b - f.y);
 }
 
-template <int KIND, bool SPLIT>
+// BF: BF16 slabs and weights (BF16 x BF16 MMAs; A and B of one MMA have the
+// same type), else FP16
+template <int KIND, bool SPLIT, bool BF>
 __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_constant__ TcParams prm)
 {
     using KT = KindTraits<KIND>;
@@ -234,8 +254,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     // TC_NMAX / 64)
     const int n_a = N16 < TC_NMAX ? N16 : TC_NMAX;
     const int n_b = N16 - n_a;
-    const uint32_t idesc_a = idesc_f16_kmaj_a_mnmaj_b(128, n_a);
-    const uint32_t idesc_b = idesc_f16_kmaj_a_mnmaj_b(128, n_b > 0 ? n_b : 16);
+    const uint32_t idesc_a = idesc_f16_kmaj_a_mnmaj_b(128, n_a, BF);
+    const uint32_t idesc_b = idesc_f16_kmaj_a_mnmaj_b(128, n_b > 0 ? n_b : 16, BF);
 
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full_b[TC_NSB], empty_b[TC_NSB], full_a[TC_NSA], rec_full[TC_NSR], rec_empty[TC_NSR];
@@ -606,13 +626,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                     const float ar = v[2 * c] * px, br = v[2 * c + 1] * px;
                     const float ai = v[2 * c] * py, bi = v[2 * c + 1] * py;
                     if constexpr (SPLIT) {
-                        words[0][c] = tc_pack(ar, br);
-                        words[1][c] = tc_pack_rem(ar, br, words[0][c]);
-                        words[2][c] = tc_pack(ai, bi);
-                        words[3][c] = tc_pack_rem(ai, bi, words[2][c]);
+                        words[0][c] = tc_pack<BF>(ar, br);
+                        words[1][c] = tc_pack_rem<BF>(ar, br, words[0][c]);
+                        words[2][c] = tc_pack<BF>(ai, bi);
+                        words[3][c] = tc_pack_rem<BF>(ai, bi, words[2][c]);
                     } else {
-                        words[0][c] = tc_pack(ar, br);
-                        words[1][c] = tc_pack(ai, bi);
+                        words[0][c] = tc_pack<BF>(ar, br);
+                        words[1][c] = tc_pack<BF>(ai, bi);
                     }
                 }
                 if (!wait_slot()) return false;

@@ -75,7 +75,7 @@ int fused_vb_occupancy(int kind, int d, int tm, int fb, int store, size_t smem);
 // per SM, all 512 tensor-memory columns): fb frames per block (multiple of
 // 8, 32..tc_max_frames_per_block(split)), slabs of rows_per_slab rows of
 // 2 fb halfs.  split = 1: weights as two FP16 terms (hi + remainder).
-cudaError_t launch_fused_tc(int kind, int split, const FusedJob &job, int fb, int rows_per_slab, int64_t n_items,
+cudaError_t launch_fused_tc(int kind, int split, int bf16, const FusedJob &job, int fb, int rows_per_slab, int64_t n_items,
                             unsigned long long *err, int n_sm, cudaStream_t st);
 int tc_max_frames_per_block(int split);
 int tc_tmem_columns(int fb, int split);

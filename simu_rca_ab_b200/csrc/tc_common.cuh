@@ -165,10 +165,11 @@ __device__ __forceinline__ uint64_t sdesc_mn_sw128(uint32_t saddr, uint32_t lbo_
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
 }
-// kind::f16, F16 x F16 -> F32, A K-major, B MN-major, M x N
-constexpr RCABF_HD uint32_t idesc_f16_kmaj_a_mnmaj_b(int m, int n)
+// kind::f16, F16 x F16 (bf16: BF16 x BF16) -> F32, A K-major, B MN-major, M x N
+constexpr RCABF_HD uint32_t idesc_f16_kmaj_a_mnmaj_b(int m, int n, bool bf16 = false)
 {
-    return (1u << 4) | (0u << 7) | (0u << 10) | (0u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
+    const uint32_t fmt = bf16 ? 1u : 0u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (0u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
            ((uint32_t)(m >> 4) << 24);
 }
 

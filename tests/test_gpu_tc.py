@@ -176,3 +176,28 @@ def test_declined_cases(c2_40):
     assert not plan_auto["kernel"].startswith("fused_tensor_core")
     assert H.rel_rms(out8.cpu().numpy(), ref8.cpu().numpy()) < 2e-4
     assert _errcount() == 0
+
+
+def test_bf16_slabs_on_the_tensor_cores(c2_40):
+    """BF16 slabs (the Doppler ensemble's other storage): BF16 x BF16 MMAs
+    with hi + remainder BF16 weights (~16 bits).  Against the SIMT kernel on
+    the same BF16 slabs, and against the FP64 oracle at BF16's storage floor
+    (-45 dB, as the SIMT BF16 tests); single-term weights are refused for
+    BF16 (8 bits would not do)."""
+    from simu_rca_ab_b200 import _lib as L
+    w, data, eng, geom, iq = c2_40
+    x = data.contiguous()
+    out, plan = _run(w, eng, geom, x, L.KERNEL_AUTO, storage=L.STORE_BF16)
+    assert plan["kernel"] == "fused_tensor_core", plan
+    assert _errcount() == 0
+    ref, plan_s = _run(w, eng, geom, x, L.KERNEL_FUSED_TMEM, storage=L.STORE_BF16)
+    assert plan_s["kernel"] == "fused_voxel_blocked_tmem"
+    o = out[:, 0].cpu().numpy()
+    rel = H.rel_rms(o, ref[:, 0].cpu().numpy())
+    pix = np.sort(np.random.default_rng(23).choice(geom.n_pix, 1024, replace=False))
+    rms, _ = H.error_db(o[:, pix], _fp64(w, data, pix))
+    print(f"BF16 slabs, tensor cores: {rms:.1f} dB vs FP64; rel RMS vs the SIMT kernel {rel:.2e}")
+    assert rel < 2e-4
+    assert rms <= -45.0
+    with pytest.raises(Exception):
+        _run(w, eng, geom, x, L.KERNEL_FUSED_TC_FP16W, storage=L.STORE_BF16)
