@@ -216,8 +216,10 @@ __device__ __forceinline__ uint32_t tc_pack(float a, float b)
     }
     return r;
 }
+// x - hi for both halves as one packed FMA (hi * -1 + x: the subtraction's
+// single rounding)
 template <bool BF>
-__device__ __forceinline__ uint32_t tc_pack_rem(float a, float b, uint32_t hi)
+__device__ __forceinline__ uint32_t tc_pack_rem(float2 x, uint32_t hi)
 {
     float2 f;
     if constexpr (BF) {
@@ -229,7 +231,8 @@ __device__ __forceinline__ uint32_t tc_pack_rem(float a, float b, uint32_t hi)
         memcpy(&h, &hi, 4);
         f = __half22float2(h);
     }
-    return tc_pack<BF>(a - f.x, b - f.y);
+    const float2 r = __ffma2_rn(f, make_float2(-1.0f, -1.0f), x);
+    return tc_pack<BF>(r.x, r.y);
 }
 
 // BF: BF16 slabs and weights (BF16 x BF16 MMAs; A and B of one MMA have the
@@ -623,16 +626,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 uint32_t words[NMAT][8];
 #pragma unroll
                 for (int c = 0; c < 8; ++c) {
-                    const float ar = v[2 * c] * px, br = v[2 * c + 1] * px;
-                    const float ai = v[2 * c] * py, bi = v[2 * c + 1] * py;
+                    // (Re, Im) of the pair's two weights: packed FP32 products
+                    const float2 vv = make_float2(v[2 * c], v[2 * c + 1]);
+                    const float2 r = __fmul2_rn(vv, make_float2(px, px));
+                    const float2 i = __fmul2_rn(vv, make_float2(py, py));
                     if constexpr (SPLIT) {
-                        words[0][c] = tc_pack<BF>(ar, br);
-                        words[1][c] = tc_pack_rem<BF>(ar, br, words[0][c]);
-                        words[2][c] = tc_pack<BF>(ai, bi);
-                        words[3][c] = tc_pack_rem<BF>(ai, bi, words[2][c]);
+                        words[0][c] = tc_pack<BF>(r.x, r.y);
+                        words[1][c] = tc_pack_rem<BF>(r, words[0][c]);
+                        words[2][c] = tc_pack<BF>(i.x, i.y);
+                        words[3][c] = tc_pack_rem<BF>(i, words[2][c]);
                     } else {
-                        words[0][c] = tc_pack<BF>(ar, br);
-                        words[1][c] = tc_pack<BF>(ai, bi);
+                        words[0][c] = tc_pack<BF>(r.x, r.y);
+                        words[1][c] = tc_pack<BF>(i.x, i.y);
                     }
                 }
                 if (!wait_slot()) return false;
