@@ -147,8 +147,8 @@ struct TcParams {
 
 // Tile coordinates of a tile index, depth slowest: the CTAs working at one
 // time hold tiles of one or two depths, whose windows of a step cover a few
-// dozen of the slab's rows, so the rows they read stay in L2 while the CTAs
-// drift apart across the steps.
+// hundred of the slab's rows, so the rows they read stay in L2 while the
+// CTAs drift apart across the steps.
 __device__ __forceinline__ void tc_tile_coords(const FusedJob &J, int64_t tile, int &tu, int &tv, int &tz)
 {
     tu = (int)(tile % J.tiles_u);
@@ -267,6 +267,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
     __shared__ volatile int last_rec[TC_NSB];   // loader: latest record loaded into each stage, -1 none
     __shared__ uint32_t tbase_s;
     __shared__ volatile int abort_s;
+    __shared__ volatile int acc_seen;   // latest item whose accumulator phase a builder group has seen complete
     uint8_t *Bs = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -296,6 +297,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
         mbar_init(&acc_empty, 128);
         mbar_init(&fin, 1);
         abort_s = 0;
+        acc_seen = -1;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -527,7 +529,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 if (!wait_slot()) break;
                 mbar_arrive(&full_a[ast]);
                 // ---- epilogue: D -> out (frames of this block) ----
+                // acc_full completes once per item.  Its parity names the
+                // item only if the previous item's phase has completed: the
+                // group of that item's end record has seen it.  (An item of
+                // fewer than two records could otherwise reach this wait
+                // while the phase of the item two back is still open.)
+                bool seen = true;
+                if (inf.it > 0 && acc_seen < inf.it - 1) {
+                    const uint64_t t0 = global_ns();
+                    while (acc_seen < inf.it - 1) {
+                        if (*abort) { seen = false; break; }
+                        if (global_ns() - t0 > 2000000000ull) { *abort = 1; seen = false; break; }
+                    }
+                }
+                if (!__all_sync(0xffffffffu, seen)) break;
                 if (!warp_wait(&acc_full, (uint32_t)inf.it & 1u, abort)) break;
+                if (m == 0) acc_seen = inf.it;
                 tmem_fence_after_sync();
                 const int64_t pix = iz * g.s_z + iu * g.s_u + iv * g.s_v;
                 for (int c = 0; c < N16; c += 16) {
