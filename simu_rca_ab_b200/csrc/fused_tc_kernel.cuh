@@ -1,5 +1,5 @@
 // Delay-and-sum on the tensor cores (sm_100a tcgen05.mma), EXACT tables,
-// FP16 slabs, rectilinear grids, transmits compounded.
+// FP16 or BF16 slabs, rectilinear grids, transmits compounded.
 //
 // Formulation.  For a tile of 128 voxels (tu along the receive axis x tv
 // along the steering axis, one depth; the planner picks the shape whose
@@ -12,8 +12,8 @@
 //     out[m][f] += sum_k W[m][k] * S[lo + k][f],
 // and summing over all (tx, rx) steps is one long contraction: the tile's
 // accumulators stay in tensor memory across the whole acquisition.  S rows
-// hold the frames of a block as (re, im) FP16 pairs, and the ingest writes a
-// second copy S' of the slabs holding (-im, re), so with the real and
+// hold the frames of a block as (re, im) FP16 (BF16) pairs, and the ingest
+// writes a second copy S' of the slabs holding (-im, re), so with the real and
 // imaginary parts of W in two matrices one accumulator takes both:
 //     D = Re(W) . S + Im(W) . S'    (N = 2 FB columns, (re, im) per frame)
 // i.e. D[re] = Re(W) S_re - Im(W) S_im, D[im] = Re(W) S_im + Im(W) S_re.
@@ -25,18 +25,21 @@
 // weights are built once per (tile, step, frame block): the builders' work
 // per frame falls as the block grows, while the MMA work per frame stays.
 // Weights are formed in FP32 exactly as the SIMT kernels form them (degree-6
-// polynomials, FP32 phasors) and enter the MMA as FP16: SPLIT = true adds a
-// second FP16 term holding the remainder (hi + lo carries ~22 bits, the MMA
+// polynomials, FP32 phasors) and enter the MMA in the slabs' type (A and B
+// of one MMA have the same type): SPLIT = true adds a second term holding
+// the remainder (hi + lo carries ~22 bits in FP16, ~16 in BF16; the MMA
 // products are exact and summed in FP32), SPLIT = false keeps the single
-// FP16 rounding (~11 bits).  All weights are scaled by 2^8 (undone in the
-// epilogue) so that the remainder terms stay out of the FP16 subnormal range.
+// FP16 rounding (~11 bits; not offered for BF16).  All weights are scaled by
+// 2^8 (undone in the epilogue) so that the remainder terms stay out of the
+// FP16 subnormal range.
 //
 // Records.  A step's window is one or two 16-row chunks; each chunk is one
 // record (one K = 16 slice of the contraction), so every record has the same
 // shape: one weight slot of NMAT matrices of 8 tensor-memory columns, one
 // window stage of 16 rows of S and of S'.
 //
-// Roles (480 threads): three groups of four warps build the weight
+// Roles (480 threads; tiles in depth-slowest order): three groups of four
+// warps build the weight
 // matrices, one voxel per thread, straight into tensor memory (lane = voxel
 // row; tcgen05.st), taking records in turn (group g the records q with
 // q mod 3 = g, so that the groups' dependent setup chains overlap), and the
