@@ -616,8 +616,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 ok = false;
                 o = 0;
             }
+            // a warp none of whose voxels has a tap in this record stores
+            // zero rows without forming weights
+            const bool warp_any = __any_sync(0xffffffffu, ok);
             float w[TAPS];
-            poly_weights<KIND, 6>(ok ? idx - fl : 0.0f, w);
+            if (warp_any) poly_weights<KIND, 6>(ok ? idx - fl : 0.0f, w);
             // P = apod e^{j phi_tx} e^{j phi_rx} e^{j phi_ab} (apod folded in (ar, ai)), scaled
             const float qx = fmaf(ptr, e.y, -pti * e.z), qy = fmaf(ptr, e.z, pti * e.y);
             const float px = ok ? TC_SCALE * fmaf(qx, abp.x, -qy * abp.y) : 0.0f;
@@ -633,31 +636,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1) fused_tc_kernel(const __grid_co
                 // clipped to the chunk (placed at o + 16 - 16 ch over 32
                 // positions, of which the upper 16 are kept; a start past
                 // the end leaves the chunk empty)
-                float v[16];
-                if constexpr (WIDE) {
-                    const int e = o + 16 - 16 * inf.ch;
-                    float v32[32];
-                    tc_place<TAPS, 32>(w, e < 32 ? e : 0, v32);
-#pragma unroll
-                    for (int p = 0; p < 16; ++p) v[p] = v32[16 + p];
-                } else {
-                    tc_place<TAPS, 16>(w, o, v);
-                }
                 uint32_t words[NMAT][8];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) {
-                    // (Re, Im) of the pair's two weights: packed FP32 products
-                    const float2 vv = make_float2(v[2 * c], v[2 * c + 1]);
-                    const float2 r = __fmul2_rn(vv, make_float2(px, px));
-                    const float2 i = __fmul2_rn(vv, make_float2(py, py));
-                    if constexpr (SPLIT) {
-                        words[0][c] = tc_pack<BF>(r.x, r.y);
-                        words[1][c] = tc_pack_rem<BF>(r, words[0][c]);
-                        words[2][c] = tc_pack<BF>(i.x, i.y);
-                        words[3][c] = tc_pack_rem<BF>(i, words[2][c]);
+                for (int mat = 0; mat < NMAT; ++mat)
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) words[mat][c] = 0u;
+                if (warp_any) {
+                    float v[16];
+                    if constexpr (WIDE) {
+                        const int e = o + 16 - 16 * inf.ch;
+                        float v32[32];
+                        tc_place<TAPS, 32>(w, e < 32 ? e : 0, v32);
+#pragma unroll
+                        for (int p = 0; p < 16; ++p) v[p] = v32[16 + p];
                     } else {
-                        words[0][c] = tc_pack<BF>(r.x, r.y);
-                        words[1][c] = tc_pack<BF>(i.x, i.y);
+                        tc_place<TAPS, 16>(w, o, v);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        // (Re, Im) of the pair's two weights: packed FP32 products
+                        const float2 vv = make_float2(v[2 * c], v[2 * c + 1]);
+                        const float2 r = __fmul2_rn(vv, make_float2(px, px));
+                        const float2 i = __fmul2_rn(vv, make_float2(py, py));
+                        if constexpr (SPLIT) {
+                            words[0][c] = tc_pack<BF>(r.x, r.y);
+                            words[1][c] = tc_pack_rem<BF>(r, words[0][c]);
+                            words[2][c] = tc_pack<BF>(i.x, i.y);
+                            words[3][c] = tc_pack_rem<BF>(i, words[2][c]);
+                        } else {
+                            words[0][c] = tc_pack<BF>(r.x, r.y);
+                            words[1][c] = tc_pack<BF>(i.x, i.y);
+                        }
                     }
                 }
                 if (!wait_slot()) return false;
