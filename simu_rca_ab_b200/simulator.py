@@ -116,6 +116,8 @@ def _element_field(dev, r_scat, ele, k, trans, c, stream):
 
 
 def _props(trans):
+    """(width, height, elevation focus, baffle, lens correction) of an array,
+    in the argument order of rcabf_sim_tx_field / rcabf_sim_rx_spectrum."""
     return (float(np.ravel(trans["ElementWidth"])[0]), float(np.ravel(trans["ElementHeight"])[0]),
             float(np.ravel(trans["ElementElevationFocus"])[0]), int(np.ravel(trans["baffle"])[0]),
             float(trans["lensCorrection"]))
@@ -177,19 +179,19 @@ def sim_us_rca(Media, TransTX, TransRX, TXSI, RXSI, Options=None, *, device=None
             L.check(lib.rcabf_sim_tx_field(
                 C.c_void_p(txf.data_ptr()), C.c_void_p(r.data_ptr()), C.c_void_p(bsc.data_ptr()),
                 C.c_void_p(ele_tx.data_ptr()), C.c_void_p(k.data_ptr()), C.c_void_p(tx_fac.data_ptr()),
-                C.c_void_p(d.data_ptr()), C.c_void_p(a.data_ptr()), G, *ptx[:4], ptx[4], c, n_scat, n_ele_tx, n_f,
-                n_sub_tx, C.c_void_p(stream)), "rcabf_sim_tx_field")
+                C.c_void_p(d.data_ptr()), C.c_void_p(a.data_ptr()), G, *ptx, c, n_scat, n_ele_tx, n_f, n_sub_tx,
+                C.c_void_p(stream)), "rcabf_sim_tx_field")
             spec = torch.empty((n_f, n_ele_rx, G), dtype=torch.complex64, device=dev)
             L.check(lib.rcabf_sim_rx_spectrum(
                 C.c_void_p(spec.data_ptr()), C.c_void_p(txf.data_ptr()), C.c_void_p(r.data_ptr()),
                 C.c_void_p(ele_rx.data_ptr()), C.c_void_p(k.data_ptr()), C.c_void_p(rx_fac.data_ptr()),
-                C.c_void_p(ra.data_ptr()), G, *prx[:4], prx[4], c, n_scat, n_ele_rx, n_f, n_sub_rx,
-                C.c_void_p(stream)), "rcabf_sim_rx_spectrum")
+                C.c_void_p(ra.data_ptr()), G, *prx, c, n_scat, n_ele_rx, n_f, n_sub_rx, C.c_void_p(stream)),
+                "rcabf_sim_rx_spectrum")
             evs = [ev[j] for j in grp]
             e0, e1 = evs[0], evs[-1] + 1
             contiguous = evs == list(range(e0, e1))
             for buf, sb, n in ((raw, sub, n_out), (rf, 0, numel)):
-                if buf is None:
+                if buf is None or n == 0:
                     continue
                 dst = buf[e0:e1] if contiguous else torch.empty((G, n_ele_rx, n), dtype=torch.float32, device=dev)
                 L.check(lib.rcabf_sim_rf(C.c_void_p(dst.data_ptr()), C.c_void_p(spec.data_ptr()),

@@ -55,6 +55,16 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
 
 
+def test_raw_length_is_the_interleave_of_the_two_subsampled_rows():
+    """Raw's fast-time length: RF(1:sub:end) and RF(2:sub:end) interleaved,
+    each cut to the shorter (SimUS_CUDARCA.m:385-386)."""
+    from simu_rca_ab_b200.simulator import _out_samples
+    for sub in (2, 4, 8):
+        for numel in range(1, 40):
+            rf = np.arange(numel)
+            assert _out_samples(numel, sub) == 2 * min(rf[0::sub].size, rf[1::sub].size), (numel, sub)
+
+
 def test_host_setups_agree():
     from simu_rca_ab_b200.simulator import sim_plan
     case = sim_case()
