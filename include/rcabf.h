@@ -128,11 +128,12 @@ typedef enum rcabf_kernel {
     /* the tensor-core kernel (sm_100a tcgen05.mma: each (tx, element) step of
        a 128-voxel tile is a banded product of the voxels' interpolation
        weights with the sample window of all frames of a block, accumulated
-       in tensor memory over the acquisition): FP16 storage, exact tables,
-       compounded output, rectilinear grids, at least 32 frames.  Weights
-       enter the MMA as an FP16 value plus its FP16 remainder (~22 bits;
-       products exact, sums FP32) -- or, with _FP16W, as one FP16 value
-       (~11 bits, half the tensor work) */
+       in tensor memory over the acquisition): FP16 or BF16 storage, exact
+       tables, compounded output, rectilinear grids, at least 32 frames
+       (frame blocks up to 208).  Weights enter the MMA in the storage's
+       type as a value plus its remainder (~22 bits in FP16, ~16 in BF16;
+       products exact, sums FP32) -- or, with _FP16W (FP16 storage only), as
+       one FP16 value (~11 bits, half the tensor work) */
     RCABF_KERNEL_FUSED_TC = 6,
     RCABF_KERNEL_FUSED_TC_FP16W = 7
 } rcabf_kernel;
