@@ -25,6 +25,7 @@ from __future__ import annotations
 import random
 from dataclasses import dataclass, field
 
+# the kernel's constants (TC_GROUPS, TC_NSA, TC_NSB, TC_NSR, TC_NPUB)
 GROUPS, NSA, NSB = 3, 3, 6
 NSR = 2 * NSB
 NPUB = NSR // 2
@@ -71,18 +72,23 @@ class Model:
     items: list             # records per item (>= 0)
     seed: int = 0
     acc_seen_wait: bool = True
+    groups: int = GROUPS    # ring sizes, the kernel's by default
+    nsa: int = NSA
+    nsb: int = NSB
+    nsr: int = NSR
+    npub: int = NPUB
     rng: random.Random = field(init=False)
 
     def __post_init__(self):
         self.rng = random.Random(self.seed)
         B = lambda n, c=1: Bar(n, c)
-        self.rec_full = [B(f"rec_full{i}") for i in range(NSR)]
-        self.rec_empty = [B(f"rec_empty{i}") for i in range(NSR)]
-        self.full_b = [B(f"full_b{i}") for i in range(NSB)]
-        self.empty_b = [B(f"empty_b{i}") for i in range(NSB)]
-        self.full_a = [B(f"full_a{i}") for i in range(NSA)]
+        self.rec_full = [B(f"rec_full{i}") for i in range(self.nsr)]
+        self.rec_empty = [B(f"rec_empty{i}") for i in range(self.nsr)]
+        self.full_b = [B(f"full_b{i}") for i in range(self.nsb)]
+        self.empty_b = [B(f"empty_b{i}") for i in range(self.nsb)]
+        self.full_a = [B(f"full_a{i}") for i in range(self.nsa)]
         self.acc_full, self.acc_empty = B("acc_full"), B("acc_empty")
-        self.info = [None] * NSR
+        self.info = [None] * self.nsr
         self.acc_seen = -1
         self.events = []            # (time, seq, fn)
         self.commit_tail = 0.0      # commits complete in issue order
@@ -93,7 +99,7 @@ class Model:
         recs = []
         for it, n in enumerate(self.items):
             recs += [(STEP, it)] * n + [(END, it)]
-        self.records = recs + [(FINAL, len(self.items))] * GROUPS
+        self.records = recs + [(FINAL, len(self.items))] * self.groups
 
     # -- asynchronous completions -------------------------------------------
     def later(self, delay, fn):
@@ -109,8 +115,8 @@ class Model:
 
     # -- roles ----------------------------------------------------------------
     def emit(self, q, rec):
-        rs = q % NSR
-        yield Wait(self.rec_empty[rs], q // NSR - 1, f"producer emit {q}")
+        rs = q % self.nsr
+        yield Wait(self.rec_empty[rs], q // self.nsr - 1, f"producer emit {q}")
         self.info[rs] = rec
         self.rec_full[rs].arrive()
 
@@ -121,10 +127,10 @@ class Model:
             if it < n_items:
                 recs = [(STEP, it)] * self.items[it] + [(END, it)]
             else:
-                recs = [(FINAL, it)] * GROUPS
-            # rounds of at most NPUB records, emitted by parallel lanes
-            for r0 in range(0, len(recs), NPUB):
-                lanes = [self.emit(q + r, recs[r]) for r in range(r0, min(r0 + NPUB, len(recs)))]
+                recs = [(FINAL, it)] * self.groups
+            # rounds of at most self.npub records, emitted by parallel lanes
+            for r0 in range(0, len(recs), self.npub):
+                lanes = [self.emit(q + r, recs[r]) for r in range(r0, min(r0 + self.npub, len(recs)))]
                 yield from self.join(lanes, "producer round")
             q += len(recs)
 
@@ -140,12 +146,12 @@ class Model:
     def loader(self):
         q = 0
         while True:
-            rs, st = q % NSR, q % NSB
-            yield Wait(self.rec_full[rs], q // NSR, f"loader rec {q}")
+            rs, st = q % self.nsr, q % self.nsb
+            yield Wait(self.rec_full[rs], q // self.nsr, f"loader rec {q}")
             kind, it = self.info[rs]
             if kind == FINAL:
                 return
-            yield Wait(self.empty_b[st], q // NSB - 1, f"loader stage {q}")
+            yield Wait(self.empty_b[st], q // self.nsb - 1, f"loader stage {q}")
             if kind == STEP:
                 self.later(self.rng.uniform(0.2, 4.0), self.full_b[st].arrive)
             else:
@@ -155,15 +161,15 @@ class Model:
     def builder(self, g):
         q = g
         while True:
-            rs = q % NSR
-            yield Wait(self.rec_full[rs], q // NSR, f"builder{g} rec {q}")
+            rs = q % self.nsr
+            yield Wait(self.rec_full[rs], q // self.nsr, f"builder{g} rec {q}")
             kind, it = self.info[rs]
             if kind == FINAL:
                 return
-            ast = q % NSA
-            if q >= NSA:                              # the slot's previous use has been consumed
-                qp = q - NSA
-                yield Wait(self.empty_b[qp % NSB], qp // NSB, f"builder{g} slot {q}")
+            ast = q % self.nsa
+            if q >= self.nsa:                              # the slot's previous use has been consumed
+                qp = q - self.nsa
+                yield Wait(self.empty_b[qp % self.nsb], qp // self.nsb, f"builder{g} slot {q}")
             self.full_a[ast].arrive()
             if kind == END:
                 if self.acc_seen_wait and it > 0:
@@ -172,18 +178,18 @@ class Model:
                 self.acc_seen = max(self.acc_seen, it)
                 self.epi_log.append(it)
                 self.acc_empty.arrive()
-            q += GROUPS
+            q += self.groups
 
     def mma(self):
         q, first = 0, True
         while True:
-            rs, bst, ast = q % NSR, q % NSB, q % NSA
-            yield Wait(self.rec_full[rs], q // NSR, f"mma rec {q}")
+            rs, bst, ast = q % self.nsr, q % self.nsb, q % self.nsa
+            yield Wait(self.rec_full[rs], q // self.nsr, f"mma rec {q}")
             kind, it = self.info[rs]
             if kind == FINAL:
                 return
-            yield Wait(self.full_b[bst], q // NSB, f"mma stage {q}")
-            yield Wait(self.full_a[ast], q // NSA, f"mma slot {q}")
+            yield Wait(self.full_b[bst], q // self.nsb, f"mma stage {q}")
+            yield Wait(self.full_a[ast], q // self.nsa, f"mma slot {q}")
             if first:
                 yield Wait(self.acc_empty, it - 1, f"mma acc_empty item {it}")
                 first = False
@@ -200,7 +206,7 @@ class Model:
     # -- scheduler --------------------------------------------------------------
     def run(self, max_steps: int = 2_000_000):
         roles = {"producer": self.producer(), "loader": self.loader(), "mma": self.mma()}
-        for g in range(GROUPS):
+        for g in range(self.groups):
             roles[f"builder{g}"] = self.builder(g)
         blocked = {}
         for name, gen in roles.items():

@@ -53,3 +53,28 @@ def test_the_epilogue_guard_is_needed():
             found = True
             break
     assert found
+
+
+def _finds_violation(**rings):
+    rng = random.Random(5)
+    for seed in range(60):
+        items = _items(rng, 30, True)
+        try:
+            Model(items, seed=seed, **rings).run()
+        except ProtocolError:
+            return True
+    return False
+
+
+@pytest.mark.parametrize("rings,why", [
+    (dict(nsa=6, nsb=3, nsr=6, npub=3), "more weight slots than window stages: a slot's previous use is "
+                                        "signalled on a stage that has moved on"),
+    (dict(nsr=6, npub=12), "producer rounds longer than the record ring: a lane waits on a slot whose "
+                           "previous record is not written yet"),
+])
+def test_ring_sizes_the_kernel_asserts_are_needed(rings, why):
+    """The kernel's static_asserts keep at least as many window stages as
+    weight slots and producer rounds no longer than the record ring (it uses
+    6 stages, 3 slots and rounds of half the ring): break either and the
+    model finds a wait outside its phase or a deadlock."""
+    assert _finds_violation(**rings), why
